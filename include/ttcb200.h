@@ -1,0 +1,141 @@
+/*
+ * ttcb200.h -- C ABI of the B200-native out-of-place tensor transposition
+ *
+ *     B_{pi(i0,i1,...,iN-1)} = alpha * A_{i0,i1,...,iN-1} + beta * B_{pi(i0,i1,...,iN-1)}
+ *
+ * Conventions (identical to TTC):
+ *   - Column-major: dimension 0 of a tensor has stride 1.
+ *   - perm[j] = the A-dimension that becomes B-dimension j; B-dimension j has extent size[perm[j]].
+ *   - lda[i] / ldb[j] are "outer sizes": stride of A-dim i is prod_{k<i} lda[k]; stride of B-dim j is
+ *     prod_{k<j} ldb[k]. Passing NULL means "dense" (lda = size, ldb[j] = size[perm[j]]).
+ *   - A and B are DEVICE pointers owned by the caller. Plans own a small device descriptor that is
+ *     created once; ttcb_transpose() itself never allocates.
+ *   - All calls return a ttcb_status; they never exit() and never trap. ttcb_last_error() returns a
+ *     thread-local message describing the last failure on the calling thread.
+ *
+ * Every entry point below names the TTC interface it replaces (file:line inside the TTC project).
+ */
+#ifndef TTCB200_H
+#define TTCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A cudaStream_t, declared without including the CUDA headers. 0/NULL = the legacy default stream. */
+typedef struct CUstream_st* ttcb_stream_t;
+
+#define TTCB_MAX_RANK 10   /* TTC's tuning database stores up to 10 dimensions (ttc.py:226-240) */
+
+/* Element types. TTC's --dataType letters map as s=float, d=double, c=float complex,
+ * z=double complex; a mixed pair "xy" means A has type x and B has type y (ttc.py:1218-1244). */
+typedef enum {
+  TTCB_S = 0, /* float                        */
+  TTCB_D = 1, /* double                       */
+  TTCB_C = 2, /* float complex  (cuFloatComplex layout: re, im)  */
+  TTCB_Z = 3  /* double complex (cuDoubleComplex layout: re, im) */
+} ttcb_dtype;
+
+typedef enum {
+  TTCB_OK = 0,
+  TTCB_ERR_INVALID_ARG = 1,   /* null plan / pointer where one is required, bad enum             */
+  TTCB_ERR_RANK = 2,          /* rank < 1 or rank > TTCB_MAX_RANK                                */
+  TTCB_ERR_BAD_PERM = 3,      /* perm is not a permutation of 0..rank-1 (ttc.py:754-758)          */
+  TTCB_ERR_BAD_LD = 4,        /* lda[i] < size[i] or ldb[j] < size[perm[j]] (ttc.py:739-746)      */
+  TTCB_ERR_DTYPE = 5,         /* unsupported A/B type pair (only s,d,c,z,sd,ds,cz,zc exist)       */
+  TTCB_ERR_ALIGN = 6,         /* a pointer is not aligned to its element size                     */
+  TTCB_ERR_CUDA = 7,          /* a CUDA runtime call failed; the message holds the CUDA error     */
+  TTCB_ERR_ALLOC = 8,         /* host or device allocation failed                                 */
+  TTCB_ERR_UNSUPPORTED = 9,   /* a size/extent beyond what the kernels index (see message)        */
+  TTCB_ERR_TIMEOUT = 10,      /* a bounded device-side wait gave up (batched mode)                */
+  TTCB_ERR_BETA = 11          /* beta given to a plan made for beta == 0, or missing when needed  */
+} ttcb_status;
+
+/* Kernel selection and schedule knobs. Every field 0 means "planner default".
+ * These are the candidate dimensions the autotuner searches (tile shape x vector width x loop
+ * order x block count), the B200 counterparts of TTC's blocking / loop order / threadsPerBlock
+ * search space (GPUtransposeGenerator.py:165-230, 258-285). */
+typedef struct {
+  int32_t kernel;        /* 0 auto, 1 = staged tile transpose, 2 = direct row copy            */
+  int32_t tile_elems;    /* target elements per shared-memory tile (tile kernel)              */
+  int32_t run_bytes;     /* target contiguous run length on each side, in bytes               */
+  int32_t vec;           /* 0 = widest legal 16-byte vectors, 1 = force scalar accesses        */
+  int32_t blocks;        /* CTAs launched (persistent grid); 0 = all tiles / occupancy bound  */
+  int32_t loop_order;    /* 0 = A-major raster of the tile grid, 1 = B-major, 2 = reverse A   */
+  int32_t streaming;     /* 0 = default (streaming stores when beta == 0), 1 = on, -1 = off     */
+  int32_t reserved[9];
+} ttcb_tuning;
+
+typedef struct ttcb_plan ttcb_plan;
+
+/* Replaces the generated TTC wrapper's per-call set-up (CUDAtranspose.py:395-429: cudaMalloc +
+ * cudaMemcpy of size/lda/ldb on every call) and the planning that ttc.py does before generating
+ * code (index fusion ttc_util.py:214-276, validation ttc.py:733-768, path choice
+ * CUDAtranspose.py:34-42). Extents are 64-bit (TTC used int, capping tensors at 2^31 elements).
+ * size[i] == 0 is allowed and yields a plan whose transpose is a no-op. */
+ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const int64_t* size,
+                             const int64_t* lda, const int64_t* ldb, ttcb_dtype type_a,
+                             ttcb_dtype type_b, int beta_nonzero, const ttcb_tuning* tuning);
+
+/* Replaces the generated entry point
+ *   extern "C" void <p>CuTranspose_<perm>_<sizes>[_bz](const TA* A, TB* B, const Talpha alpha,
+ *        [const Tbeta beta,] const int* size, const int* lda, const int* ldb)
+ * (CUDAtranspose.py:438-451, named at :473-527). Stream-ordered and asynchronous; it never
+ * allocates and never synchronizes. alpha points to one value of A's precision: float for s/sd,
+ * double for d/ds, {float re, im} for c/cz, {double re, im} for z/zc (TTC takes a real alpha; a
+ * complex one is an extension). beta likewise in B's precision; it is ignored (may be NULL) for a
+ * plan created with beta_nonzero == 0. */
+ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const void* alpha,
+                           const void* beta, ttcb_stream_t stream);
+
+/* Frees the plan's device descriptor. Safe on NULL. */
+void ttcb_plan_destroy(ttcb_plan* plan);
+
+/* One-line JSON description of a plan (fused problem, chosen kernel, tile, vectors, grid).
+ * Writes at most len bytes including the terminating NUL; returns the full length needed. */
+size_t ttcb_plan_describe(const ttcb_plan* plan, char* buf, size_t len);
+
+/* Algorithmic bytes of one call: N*(sizeof(TA) + sizeof(TB)*(1 + [beta != 0])), N = prod size,
+ * the bandwidth convention of GPUtransposeGenerator.py:589-592 (padding excluded). */
+int64_t ttcb_plan_bytes(const ttcb_plan* plan);
+
+/* Message of the last failure on this thread ("" if none). Replaces ttc_util.py:135-141, which
+ * printed the CUDA error and called exit(-1). */
+const char* ttcb_last_error(void);
+
+/* Library version {major, minor, patch}. */
+void ttcb_version(int* major, int* minor, int* patch);
+
+/* ---------------------------------------------------------------------------------------------
+ * Batched mode: many independent transpositions in one persistent launch.
+ * No counterpart in TTC, which can only call one generated wrapper per transposition (each with its
+ * own cudaMalloc/cudaMemcpy/cudaDeviceSynchronize, CUDAtranspose.py:395-429). The batch owns a
+ * device table of per-problem descriptors, a prefix sum of tile counts and a work counter.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ttcb_batch ttcb_batch;
+
+/* Builds a batch from already-created plans (each keeps its own schedule; the batch copies what
+ * it needs, so the plans may be destroyed afterwards). A[i]/B[i] are device pointers bound now. */
+ttcb_status ttcb_batch_create(ttcb_batch** batch, int count, const ttcb_plan* const* plans,
+                              const void* const* A, void* const* B, const void* alpha,
+                              const void* beta, int blocks);
+
+/* Runs every problem of the batch in one persistent kernel launch on stream. */
+ttcb_status ttcb_batch_launch(ttcb_batch* batch, ttcb_stream_t stream);
+
+/* Captures the batch launch (counter reset + kernel) into a CUDA graph once and replays it. */
+ttcb_status ttcb_batch_graph_launch(ttcb_batch* batch, ttcb_stream_t stream);
+
+/* Device status word of the last launch: 0 = ok, otherwise a TTCB_ERR_* code set on the device. */
+ttcb_status ttcb_batch_status(ttcb_batch* batch, ttcb_stream_t stream);
+
+int64_t ttcb_batch_bytes(const ttcb_batch* batch);
+void ttcb_batch_destroy(ttcb_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TTCB200_H */

@@ -1,0 +1,177 @@
+"""CPU replay of the kernels' index arithmetic from a plan's descriptor bytes.
+
+The planner (libttcb200.so, host code) emits the same descriptor the GPU kernels read. This module
+parses it and replays, in numpy, which A element each kernel reads and which B element it writes -
+tile decode, ragged limits, A/B run segments, shared-memory slots, row-copy units. Tests compare the
+resulting element mapping with the oracle's, so the index math is checked without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ttc_b200 import _native
+from ttc_b200._native import Tuning, i32, i64
+
+_layout = None
+
+
+def layout():
+    global _layout
+    if _layout is None:
+        a = (ctypes.c_int64 * 11)()
+        _native.lib().ttcb_test_desc_layout(a)
+        keys = ["tile_size", "off_divLA", "off_g", "g_size", "off_bd", "bd_size", "row_size", "row_off_div",
+                "row_off_sA", "row_off_sB", "fastdiv_size"]
+        _layout = dict(zip(keys, list(a)))
+    return _layout
+
+
+def host_desc(perm, size, dtype="s", beta=False, lda=None, ldb=None, tuning=None):
+    """Returns (kernel kind, descriptor bytes) from the host-only planner."""
+    ta, tb = (dtype[0], dtype[1]) if len(dtype) == 2 else (dtype, dtype)
+    if isinstance(tuning, dict):
+        tuning = Tuning.make(**tuning)
+    kind = ctypes.c_int()
+    args = (len(size), i32(perm), i64(size), i64(lda) if lda else None, i64(ldb) if ldb else None,
+            _native.DTYPES[ta], _native.DTYPES[tb], int(beta), ctypes.byref(tuning) if tuning else None,
+            ctypes.byref(kind))
+    n = _native.lib().ttcb_test_plan_host_desc(*args, None, 0)
+    if n == 0:
+        raise _native.TTCError(1, _native.last_error())
+    buf = ctypes.create_string_buffer(n)
+    _native.lib().ttcb_test_plan_host_desc(*args, buf, n)
+    return kind.value, buf.raw
+
+
+def _i32(b, off):
+    return int(np.frombuffer(b, dtype=np.int32, count=1, offset=off)[0])
+
+
+def _i64(b, off):
+    return int(np.frombuffer(b, dtype=np.int64, count=1, offset=off)[0])
+
+
+def _fd(b, off):
+    d, m, l, _ = np.frombuffer(b, dtype=np.uint32, count=4, offset=off)
+    return int(d), int(m), int(l)
+
+
+def fdiv(n, fd):
+    """The kernels' division by invariant integer, bit for bit (32-bit arithmetic)."""
+    d, m, l = fd
+    n = np.asarray(n, dtype=np.uint64)
+    hi = (n * np.uint64(m)) >> np.uint64(32)
+    return ((hi + n) & np.uint64(0xFFFFFFFF)) >> np.uint64(l)
+
+
+def parse_tile(b):
+    L = layout()
+    names = ["P", "LA", "LB", "nsegA", "nsegB", "pshift", "pad", "phys_size", "ngrid", "nblocked", "ntiles",
+             "off_segA", "off_segB", "off_perm", "smem_bytes"]
+    t = {k: _i32(b, 4 * i) for i, k in enumerate(names)}
+    t["divLA"] = _fd(b, L["off_divLA"])
+    t["divLB"] = _fd(b, L["off_divLA"] + L["fastdiv_size"])
+    g = []
+    for k in range(t["ngrid"]):
+        o = L["off_g"] + k * L["g_size"]
+        g.append({"div": _fd(b, o), "strideA": _i64(b, o + 16), "strideB": _i64(b, o + 24), "n": _i64(b, o + 32),
+                  "e": _i32(b, o + 40), "blocked": _i32(b, o + 44)})
+    t["g"] = g
+    bd = []
+    for k in range(t["nblocked"]):
+        o = L["off_bd"] + k * L["bd_size"]
+        bd.append({"tsA": _fd(b, o), "tsB": _fd(b, o + 16), "ext": _fd(b, o + 32)})
+    t["bd"] = bd
+    t["segA"] = np.frombuffer(b, dtype=np.int64, count=t["nsegA"], offset=t["off_segA"])
+    t["segB"] = np.frombuffer(b, dtype=np.int64, count=t["nsegB"], offset=t["off_segB"])
+    t["ptab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_perm"]).astype(np.int64)
+    return t
+
+
+def parse_row(b):
+    L = layout()
+    r = {"w": _i64(b, 0), "chunk": _i32(b, 8), "nchunk": _i32(b, 12), "nd": _i32(b, 16), "nunits": _i32(b, 20),
+         "divChunk": _fd(b, 24)}
+    r["div"] = [_fd(b, L["row_off_div"] + 16 * k) for k in range(r["nd"])]
+    r["sA"] = [_i64(b, L["row_off_sA"] + 8 * k) for k in range(r["nd"])]
+    r["sB"] = [_i64(b, L["row_off_sB"] + 8 * k) for k in range(r["nd"])]
+    return r
+
+
+def simulate_tile(t):
+    """Returns arrays (a_off, b_off): for every element written, the A element read."""
+    P = t["P"]
+    p = np.arange(P, dtype=np.int64)
+    q = np.arange(P, dtype=np.int64)
+    slot_q = q + ((q >> t["pshift"]) if t["pad"] else 0)
+    sA = fdiv(p, t["divLA"]).astype(np.int64)
+    a_rel = t["segA"][sA] + (p - sA * t["LA"])
+    sB = fdiv(q, t["divLB"]).astype(np.int64)
+    b_rel = t["segB"][sB] + (q - sB * t["LB"])
+    phys = int(slot_q.max()) + 1 if P else 0
+    assert phys == t["phys_size"], (phys, t["phys_size"])
+    assert len(np.unique(t["ptab"])) == P, "two elements share a shared-memory slot"
+    assert set(t["ptab"].tolist()) == set(slot_q.tolist()), "load and store slots differ"
+    a_out, b_out = [], []
+    for tile in range(t["ntiles"]):
+        rem = tile
+        bA = bB = 0
+        lim = [1 << 31, 1 << 31]
+        for g in t["g"]:
+            qq = int(fdiv(rem, g["div"]))
+            blk = rem - qq * g["div"][0]
+            rem = qq
+            bA += blk * g["strideA"]
+            bB += blk * g["strideB"]
+            if g["blocked"] >= 0:
+                lim[g["blocked"]] = min(g["e"], g["n"] - blk * g["e"])
+        okA = np.ones(P, bool)
+        okB = np.ones(P, bool)
+        for k, bd in enumerate(t["bd"]):
+            c = fdiv(p, bd["tsA"]).astype(np.int64)
+            c = c - fdiv(c, bd["ext"]).astype(np.int64) * bd["ext"][0]
+            okA &= c < lim[k]
+            c = fdiv(q, bd["tsB"]).astype(np.int64)
+            c = c - fdiv(c, bd["ext"]).astype(np.int64) * bd["ext"][0]
+            okB &= c < lim[k]
+        # slot -> A offset written in the load phase
+        slot_to_a = np.full(phys, -1, np.int64)
+        slot_to_a[t["ptab"][okA]] = bA + a_rel[okA]
+        src = slot_to_a[slot_q[okB]]
+        assert (src >= 0).all(), "store phase reads a slot the load phase did not write"
+        a_out.append(src)
+        b_out.append(bB + b_rel[okB])
+    return np.concatenate(a_out) if a_out else np.zeros(0, np.int64), \
+        np.concatenate(b_out) if b_out else np.zeros(0, np.int64)
+
+
+def simulate_row(r):
+    a_out, b_out = [], []
+    for u in range(r["nunits"]):
+        row = int(fdiv(u, r["divChunk"]))
+        ck = u - row * r["nchunk"]
+        rem = row
+        oA = oB = 0
+        for k in range(r["nd"]):
+            qq = int(fdiv(rem, r["div"][k]))
+            c = rem - qq * r["div"][k][0]
+            rem = qq
+            oA += c * r["sA"][k]
+            oB += c * r["sB"][k]
+        e0 = ck * r["chunk"]
+        e1 = min(e0 + r["chunk"], r["w"])
+        e = np.arange(e0, e1, dtype=np.int64)
+        a_out.append(oA + e)
+        b_out.append(oB + e)
+    return np.concatenate(a_out), np.concatenate(b_out)
+
+
+def simulate(perm, size, dtype="s", beta=False, lda=None, ldb=None, tuning=None):
+    kind, b = host_desc(perm, size, dtype, beta, lda, ldb, tuning)
+    if kind == 1:
+        return kind, simulate_tile(parse_tile(b))
+    if kind == 2:
+        return kind, simulate_row(parse_row(b))
+    return kind, (np.zeros(0, np.int64), np.zeros(0, np.int64))

@@ -1,0 +1,78 @@
+"""Batched mode on the GPU: every problem of a persistent launch (plain and graph-replayed) must equal
+the per-call plain kernel and the oracle bit for bit."""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import assert_bitexact, uniform
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(seed, count):
+    import ttc_b200.workloads as wl
+    return wl.batched_cases(seed=seed, count=count, median=4096, lo=64, hi=1 << 16)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_matches_oracle_and_plain_calls(graph):
+    import torch
+    from ttc_b200 import Plan
+    from ttc_b200.batched import Batch
+    cases = _problems(5, 300)
+    plans, As, Bs, Cs, wants = [], [], [], [], []
+    for k, c in enumerate(cases):
+        n = int(np.prod(c["size"]))
+        a = uniform(n, "s", 100 + k)
+        wants.append(oracle.transpose(a, np.zeros(n, np.float32), c["perm"], c["size"], 1.0, 0.0, dtype="s"))
+        plans.append(Plan(c["perm"], c["size"], "s"))
+        As.append(torch.from_numpy(a).cuda())
+        Bs.append(torch.full((n,), float("nan"), device="cuda"))
+        Cs.append(torch.full((n,), float("nan"), device="cuda"))
+    batch = Batch(plans, As, Bs, alpha=1.0)
+    for rep in range(2):  # the second launch re-runs on reset counters
+        batch.launch(graph=graph)
+    batch.check_status()
+    for p, a, cbuf in zip(plans, As, Cs):
+        p(a, cbuf, 1.0)
+    torch.cuda.synchronize()
+    for k, (b, cbuf, w) in enumerate(zip(Bs, Cs, wants)):
+        assert_bitexact(b.cpu().numpy(), w, f"batched problem {k} {cases[k]}")
+        assert torch.equal(b, cbuf)
+
+
+def test_batched_beta_mixed_kernels_and_dtypes():
+    import torch
+    from ttc_b200 import Plan
+    from ttc_b200.batched import Batch
+    rng = np.random.default_rng(3)
+    for dtype in ("d", "zc", "sd"):
+        ta, tb = (dtype[0], dtype[1]) if len(dtype) == 2 else (dtype, dtype)
+        tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
+        plans, As, Bs, wants = [], [], [], []
+        for k in range(40):
+            r = int(rng.integers(2, 5))
+            size = [int(x) for x in rng.integers(1, 40, r)]
+            perm = [int(x) for x in rng.permutation(r)]
+            n = int(np.prod(size))
+            a = uniform(n, ta, k)
+            b = uniform(n, tb, 1000 + k)
+            alpha, beta = (complex(0.5, -1.0), complex(2.0, 0.25)) if ta in "cz" else (0.5, 2.0)
+            wants.append(oracle.transpose(a, b.copy(), perm, size, alpha, beta, dtype=dtype))
+            plans.append(Plan(perm, size, dtype, True, tuning={"vec": k % 2}))
+            As.append(torch.from_numpy(a).cuda())
+            Bs.append(torch.from_numpy(b).cuda())
+        Batch(plans, As, Bs, alpha=alpha, beta=beta).launch()
+        torch.cuda.synchronize()
+        for k, (bb, w) in enumerate(zip(Bs, wants)):
+            assert_bitexact(bb.cpu().numpy(), w, f"{dtype} problem {k}")
+
+
+def test_batch_rejects_mixed_types():
+    from ttc_b200 import Plan, TTCError
+    from ttc_b200.batched import Batch
+    import torch
+    x = torch.zeros(64, device="cuda", dtype=torch.float64)
+    y = torch.zeros(64, device="cuda", dtype=torch.float32)
+    with pytest.raises(TTCError):
+        Batch([Plan([1, 0], [8, 8], "s"), Plan([1, 0], [8, 8], "d")], [y, x], [y, x])

@@ -1,0 +1,201 @@
+"""GPU parity: the sm_100a kernels against the CPU oracle, bit for bit.
+
+Every kernel rounds each product and sum once (explicitly rounded intrinsics), like the oracle
+compiled without contraction, so the bar is bit-exact for every dtype pair and alpha/beta - stricter
+than the <= 1 ulp the contracted reference would allow.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import (assert_bitexact, make_inputs, split, ttc_cases, uniform, NP, buffer_len)
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def run_gpu(A, B, perm, size, dtype, alpha, beta, lda=None, ldb=None, tuning=None, offset=0):
+    """Runs the library on copies of A and B; offset shifts both buffers by elements (alignment)."""
+    torch = _torch()
+    from ttc_b200 import Plan
+    ta, tb = split(dtype)
+    tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
+    dA = torch.empty(A.size + offset, dtype=tmap[ta], device="cuda")
+    dB = torch.empty(B.size + offset + 64, dtype=tmap[tb], device="cuda")
+    dA[offset:].copy_(torch.from_numpy(A))
+    dB[offset:offset + B.size].copy_(torch.from_numpy(B))
+    canary = torch.from_numpy(uniform(64, tb, 99))
+    dB[offset + B.size:].copy_(canary)
+    plan = Plan(perm, size, dtype, complex(beta) != 0, lda, ldb, tuning)
+    plan(dA[offset:], dB[offset:], alpha, beta)
+    torch.cuda.synchronize()
+    out = dB[offset:offset + B.size].cpu().numpy()
+    tail = dB[offset + B.size:].cpu().numpy()
+    assert np.array_equal(tail.view(np.uint8), canary.numpy().view(np.uint8)), "write past the end of B"
+    desc = plan.describe()
+    plan.close()
+    return out, desc
+
+
+def check_case(perm, size, dtype, alpha, beta, lda=None, ldb=None, tuning=None, seed=7, offset=0):
+    A, B = make_inputs(size, perm, dtype, seed, lda, ldb)
+    want = oracle.transpose(A, B.copy(), perm, size, alpha, beta, lda, ldb, dtype)
+    got, desc = run_gpu(A, B, perm, size, dtype, alpha, beta, lda, ldb, tuning, offset)
+    assert_bitexact(got, want, f"perm={perm} size={size} dtype={dtype} a={alpha} b={beta} lda={lda} "
+                               f"ldb={ldb} tuning={tuning} plan={desc}")
+    return desc
+
+
+def test_ttc_reference_case_matrix():
+    """The reference's own sweep (test-framework/ttc_test.py:80-217) on the GPU path."""
+    for perm, size, dtype, alpha, beta in ttc_cases():
+        check_case(perm, size, dtype, alpha, beta)
+
+
+def test_readme_shape_full_size():
+    """perm 1,0,2 / 1000x768x16 fp32, alpha = beta = 1 (the README example)."""
+    desc = check_case([1, 0, 2], [1000, 768, 16], "s", 1.0, 1.0)
+    assert desc["kernel"] == "tile"
+    check_case([1, 0, 2], [1000, 768, 16], "s", 1.0, 0.0)
+
+
+@pytest.mark.parametrize("dtype,alpha", [("zc", complex(0.5, 0.25)), ("ds", 0.5), ("z", complex(0.5, 0.25)),
+                                         ("d", 0.5)])
+def test_strided_mixed_precision_config(dtype, alpha):
+    """rank-4 perm 3,1,0,2, extents 96,80,72,64, lda = extents + {8,0,4,0}, B dense, beta = 0."""
+    check_case([3, 1, 0, 2], [96, 80, 72, 64], dtype, alpha, 0.0, lda=[104, 80, 76, 64])
+
+
+@pytest.mark.parametrize("dtype", ["s", "d", "c", "z", "sd", "ds", "cz", "zc"])
+def test_padded_lda_ldb_and_complex_beta(dtype):
+    ta, tb = split(dtype)
+    cplx = ta in "cz"
+    alpha = complex(1.25, -0.75) if cplx else 1.25
+    beta = complex(-0.5, 0.3) if cplx else -0.5
+    check_case([2, 0, 3, 1], [13, 9, 6, 11], dtype, alpha, beta, lda=[16, 10, 6, 12], ldb=[6, 15, 9, 11])
+    check_case([1, 2, 0], [33, 17, 9], dtype, alpha, 0.0, ldb=[17, 12, 33])
+
+
+TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"blocks": 7}, {"tile_elems": 512},
+           {"tile_elems": 8192}, {"run_bytes": 128}, {"run_bytes": 2048}, {"kernel": 1}, {"streaming": -1},
+           {"streaming": 1}]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS, ids=[str(t) for t in TUNINGS])
+def test_schedule_knobs_do_not_change_results(tuning):
+    for perm, size in ([[1, 0, 2], [300, 257, 5]], [[2, 0, 1], [7, 3, 20001]], [[0, 2, 1], [40, 33, 17]],
+                       [[4, 2, 0, 3, 1], [9, 11, 7, 13, 5]], [[0, 1], [1000, 77]]):
+        for dtype, beta in (("s", 0.0), ("d", 1.5), ("c", 0.0)):
+            try:
+                check_case(perm, size, dtype, 1.5, beta, tuning=tuning)
+            except Exception as e:  # a forced tile kernel may not apply to every problem
+                if "TTCB_ERR_UNSUPPORTED" in str(e) and tuning.get("kernel"):
+                    continue
+                raise
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3])
+def test_misaligned_pointers_fall_back_to_narrow_accesses(offset):
+    check_case([1, 0, 2], [64, 96, 3], "s", 1.0, 0.5, offset=offset)
+    check_case([0, 2, 1], [256, 7, 9], "s", 2.0, 0.0, offset=offset)
+    check_case([1, 0], [40, 33], "d", 1.0, 1.0, offset=offset)
+
+
+def test_random_problems_ranks_1_to_6():
+    rng = np.random.default_rng(11)
+    for it in range(120):
+        r = int(rng.integers(1, 7))
+        size = [int(x) for x in rng.integers(1, 14, r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        dtype = ["s", "d", "c", "z", "sd", "ds", "cz", "zc"][it % 8]
+        beta = [0.0, 1.0, -0.5][it % 3]
+        lda = [s + int(rng.integers(0, 2)) for s in size] if it % 4 == 0 else None
+        check_case(perm, size, dtype, 1.5, beta, lda=lda, seed=it)
+
+
+def test_edge_values_and_signed_zero():
+    """Values that expose sign, rounding and special-value handling (NaN, inf, -0, denormals)."""
+    torch = _torch()
+    perm, size = [1, 0], [37, 41]
+    for dtype in ("s", "d", "ds", "sd"):
+        ta, tb = split(dtype)
+        A, B = make_inputs(size, perm, dtype, 3)
+        special = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 1e-40, -1e-310, 3.4e38, 1.0 + 2**-23],
+                           dtype=np.float64)
+        A[: special.size] = special.astype(A.dtype)
+        B[-special.size:] = special.astype(B.dtype)
+        for alpha, beta in ((1.0, 0.0), (-1.0, 1.0), (3.0, -2.0)):
+            want = oracle.transpose(A, B.copy(), perm, size, alpha, beta, dtype=dtype)
+            got, _ = run_gpu(A, B, perm, size, dtype, alpha, beta)
+            assert_bitexact(got, want, f"special {dtype} {alpha} {beta}")
+
+
+def test_empty_and_single_element():
+    check_case([0], [1], "s", 2.0, 1.0)
+    check_case([1, 0], [1, 1], "z", complex(2, 1), 0.0)
+    from ttc_b200 import Plan
+    torch = _torch()
+    p = Plan([1, 0], [0, 5], "s")
+    x = torch.zeros(4, device="cuda")
+    p(x, x, 1.0)  # no-op
+    torch.cuda.synchronize()
+
+
+def test_error_paths_do_not_poison_the_context():
+    import ctypes
+    from ttc_b200 import Plan, TTCError
+    from ttc_b200._native import check, lib
+    torch = _torch()
+    x = torch.zeros(64, device="cuda")
+    y = torch.zeros(64, device="cuda")
+    p0 = Plan([1, 0], [8, 8], "s", beta_nonzero=False)
+    with pytest.raises(TTCError) as e:
+        p0(x, y, 1.0, 0.5)  # beta given to a plan made for beta == 0
+    assert e.value.code == "TTCB_ERR_BETA"
+    with pytest.raises(TTCError) as e:
+        Plan([1, 0], [8, 8], "s", lda=[4, 8])
+    assert e.value.code == "TTCB_ERR_BAD_LD"
+    with pytest.raises(TTCError) as e:
+        Plan([0, 0], [8, 8], "s")
+    assert e.value.code == "TTCB_ERR_BAD_PERM"
+    al = (ctypes.c_float * 1)(1.0)
+    with pytest.raises(TTCError) as e:  # A not aligned to its element size
+        check(lib().ttcb_transpose(p0.handle, x.data_ptr() + 2, y.data_ptr(), ctypes.cast(al, ctypes.c_void_p),
+                                   None, None))
+    assert e.value.code == "TTCB_ERR_ALIGN"
+    p1 = Plan([1, 0], [8, 8], "s", beta_nonzero=True)
+    with pytest.raises(TTCError) as e:  # beta missing for a beta != 0 plan
+        check(lib().ttcb_transpose(p1.handle, x.data_ptr(), y.data_ptr(), ctypes.cast(al, ctypes.c_void_p),
+                                   None, None))
+    assert e.value.code == "TTCB_ERR_BETA"
+    # the context is still healthy
+    check_case([1, 0], [8, 8], "s", 1.0, 0.0)
+
+
+def test_torch_permute_agrees_on_large_sweep_shapes():
+    """Size-independent property at full size: for alpha = 1, beta = 0 the result is a pure
+    permutation, identical to torch.permute(...).contiguous() bit for bit."""
+    torch = _torch()
+    from ttc_b200 import Plan
+    import ttc_b200.workloads as wl
+    cases = wl.sweep_cases(seed=2024)[:6]
+    for c in cases:
+        size, perm = c["size"], c["perm"]
+        tdt = torch.float32 if c["dtype"] == "s" else torch.float64
+        n = int(np.prod(size))
+        A = torch.rand(n, dtype=tdt, device="cuda") * 2 - 1
+        B = torch.empty_like(A)
+        p = Plan(perm, size, c["dtype"], False)
+        p(A, B, 1.0, 0.0)
+        # A viewed row-major with reversed dims; B's dims are A's dims in perm order
+        At = A.view(*reversed(size))
+        nd = len(size)
+        want = At.permute(*[nd - 1 - perm[j] for j in reversed(range(nd))]).contiguous().view(-1)
+        torch.cuda.synchronize()
+        assert torch.equal(B, want), (perm, size, p.describe())
+        del A, B, At, want
+        torch.cuda.empty_cache()

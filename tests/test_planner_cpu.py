@@ -1,0 +1,160 @@
+"""Host-side tests of the planner in libttcb200.so (no GPU): fast division, index fusion against
+TTC's fuseIndices, validation errors, and a CPU replay of the kernels' index arithmetic from the
+descriptor tables against the oracle's element mapping."""
+import itertools
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import kernel_sim
+import oracle.ttc_ref as ref
+from ttc_b200 import TTCError, fuse, plan_host_json
+from ttc_b200 import _native
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_library_exports_every_header_symbol():
+    header = (ROOT / "include" / "ttcb200.h").read_text()
+    declared = set(re.findall(r"\b(ttcb_[a-z_]+)\s*\(", header))
+    declared -= {"ttcb_stream_t"}
+    assert declared, "no declarations found"
+    lib = _native.lib()
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    assert declared == {n for n, _, _ in _native.PUBLIC_SYMBOLS}
+
+
+def test_fastdiv_matches_integer_division():
+    rng = np.random.default_rng(0)
+    divisors = list(range(1, 300)) + [int(x) for x in rng.integers(1, 2**31 - 1, 300)] + [2**k for k in range(31)]
+    nums = [0, 1, 2, 3, 2**31 - 1, 2**31 - 2, 2**30] + [int(x) for x in rng.integers(0, 2**31 - 1, 40)]
+    f = _native.lib().ttcb_test_fastdiv
+    for d in divisors:
+        for n in nums + [d - 1, d, d + 1, 3 * d, 3 * d - 1]:
+            if 0 <= n < 2**31:
+                assert f(n, d) == n // d, (n, d)
+                assert int(kernel_sim.fdiv(n, (d, *_fd(d)))) == n // d
+
+
+def _fd(d):
+    l = 0
+    while (1 << l) < d:
+        l += 1
+    m = ((((1 << l) - d) << 32) // d + 1) & 0xFFFFFFFF
+    return m, l
+
+
+def _random_problem(rng, max_rank=6, max_ext=9, pad=True, allow_one=False):
+    r = int(rng.integers(1, max_rank + 1))
+    lo = 1 if allow_one else 2
+    size = [int(x) for x in rng.integers(lo, max_ext + 1, r)]
+    perm = [int(x) for x in rng.permutation(r)]
+    lda = ldb = None
+    if pad and rng.random() < 0.5:
+        lda = [s + int(rng.integers(0, 3)) for s in size]
+    if pad and rng.random() < 0.5:
+        ldb = [size[p] + int(rng.integers(0, 3)) for p in perm]
+    return perm, size, lda, ldb
+
+
+def test_fusion_matches_ttc_fuse_indices():
+    rng = np.random.default_rng(1)
+    for _ in range(400):
+        perm, size, lda, ldb = _random_problem(rng, pad=True)
+        sA, sB = ref.strides(size, perm, lda, ldb)
+        fp, fn, fa, fb = fuse(perm, size, sA, sB)
+        rs, rp, rla, rldb = ref.fuse_indices(size, perm, lda, ldb)
+        rsA, rsB = ref.strides(rs, rp, rla, rldb)
+        assert (fp, fn) == (rp, rs), (perm, size, lda, ldb)
+        assert fa == rsA and fb == rsB, (perm, size, lda, ldb)
+
+
+def _oracle_pairs(perm, size, lda, ldb):
+    sA, sB = ref.strides(size, perm, lda, ldb)
+    grids = np.meshgrid(*[np.arange(s, dtype=np.int64) for s in size], indexing="ij")
+    a = sum(g * s for g, s in zip(grids, sA)).reshape(-1)
+    b = sum(g * s for g, s in zip(grids, sB)).reshape(-1)
+    return a, b
+
+
+TUNINGS = [None, {"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"tile_elems": 256}, {"tile_elems": 8192},
+           {"run_bytes": 128}, {"run_bytes": 1024}, {"kernel": 1}]
+
+
+def test_kernel_index_math_replay_matches_oracle_mapping():
+    rng = np.random.default_rng(2)
+    n = 0
+    for it in range(260):
+        perm, size, lda, ldb = _random_problem(rng, max_rank=5, max_ext=13, allow_one=(it % 5 == 0))
+        dtype = ["s", "d", "c", "z", "sd", "ds", "cz", "zc"][it % 8]
+        tuning = TUNINGS[it % len(TUNINGS)]
+        try:
+            kind, (a, b) = kernel_sim.simulate(perm, size, dtype, bool(it % 2), lda, ldb, tuning)
+        except TTCError:
+            if tuning and tuning.get("kernel") == 1:
+                continue  # some problems have no tile shape under a forced knob
+            raise
+        wa, wb = _oracle_pairs(perm, size, lda, ldb)
+        assert len(b) == len(wb), (perm, size, lda, ldb, dtype, tuning)
+        assert len(np.unique(b)) == len(b), "a B element is written twice"
+        got = dict(zip(b.tolist(), a.tolist()))
+        want = dict(zip(wb.tolist(), wa.tolist()))
+        assert got == want, (perm, size, lda, ldb, dtype, tuning, kind)
+        n += 1
+    assert n > 200
+
+
+@pytest.mark.parametrize("perm,size,lda,ldb", [
+    ([1, 0, 2], [1000, 768, 16], None, None),
+    ([3, 1, 0, 2], [96, 20, 18, 16], [104, 20, 19, 16], None),
+    ([2, 0, 1], [7, 3, 3000], None, None),
+    ([1, 0, 2], [20, 20, 700], None, None),
+    ([0, 2, 1], [11, 8, 300], None, None),
+    ([4, 2, 0, 3, 1], [9, 11, 7, 13, 5], None, None),
+    ([0, 1, 2], [10, 20, 30], [12, 20, 30], [10, 22, 30]),
+])
+def test_replay_larger_shapes(perm, size, lda, ldb):
+    for tuning in (None, {"vec": 1}, {"loop_order": 1}):
+        kind, (a, b) = kernel_sim.simulate(perm, size, "s", True, lda, ldb, tuning)
+        wa, wb = _oracle_pairs(perm, size, lda, ldb)
+        order = np.argsort(b)
+        worder = np.argsort(wb)
+        assert np.array_equal(b[order], wb[worder])
+        assert np.array_equal(a[order], wa[worder])
+
+
+def test_validation_errors():
+    with pytest.raises(TTCError) as e:
+        plan_host_json([0, 0, 1], [3, 4, 5])
+    assert e.value.code == "TTCB_ERR_BAD_PERM"
+    with pytest.raises(TTCError) as e:
+        plan_host_json([1, 0], [3, 4], lda=[2, 4])
+    assert e.value.code == "TTCB_ERR_BAD_LD"
+    with pytest.raises(TTCError) as e:
+        plan_host_json([1, 0], [3, 4], ldb=[3, 4])
+    assert e.value.code == "TTCB_ERR_BAD_LD"
+    with pytest.raises(TTCError) as e:
+        plan_host_json(list(range(11)), [2] * 11)
+    assert e.value.code == "TTCB_ERR_RANK"
+    with pytest.raises(TTCError):
+        plan_host_json([1, 0], [3, 4], dtype="sc")
+
+
+def test_planner_choices_for_reference_shapes():
+    j = plan_host_json([1, 0, 2], [1000, 768, 16], "s", True)
+    assert j["kernel"] == "tile" and j["vecA"] == 4 and j["vecB"] == 4
+    assert j["tile"]["LA"] * 4 >= 128 and j["tile"]["LB"] * 4 >= 128
+    j = plan_host_json([0, 2, 1], [1000, 50, 60], "s", False)
+    assert j["kernel"] == "row"
+    j = plan_host_json([0, 1, 2], [10, 20, 30], "d", False)
+    assert j["kernel"] == "row" and j["fused"]["rank"] == 1
+    j = plan_host_json([1, 0, 2], [20, 20, 100000], "s", False)
+    assert j["tile"]["LA"] >= 400 and j["tile"]["LB"] >= 400  # whole 20x20 planes per tile
+    j = plan_host_json([3, 1, 0, 2], [96, 80, 72, 64], "zc", False, lda=[104, 80, 76, 64])
+    assert j["kernel"] == "tile"
+    # empty tensors are a no-op plan
+    j = plan_host_json([1, 0], [0, 5], "s", False)
+    assert j["elements"] == 0

@@ -1,0 +1,331 @@
+// C ABI of the plain transposition: plan creation (validation, fusion, descriptor upload),
+// asynchronous execution, error reporting.
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/ttcb200.h"
+#include "kernels.cuh"
+#include "launch.h"
+#include "plan.h"
+#include "testing.h"
+
+namespace ttcb {
+KernelRef pick_kernel_ss(int, int, int, int);
+KernelRef pick_kernel_dd(int, int, int, int);
+KernelRef pick_kernel_cc(int, int, int, int);
+KernelRef pick_kernel_zz(int, int, int, int);
+KernelRef pick_kernel_sd(int, int, int, int);
+KernelRef pick_kernel_ds(int, int, int, int);
+KernelRef pick_kernel_cz(int, int, int, int);
+KernelRef pick_kernel_zc(int, int, int, int);
+
+KernelRef pick_kernel(ttcb_dtype ta, ttcb_dtype tb, int kernel, int va, int vb, int variant) {
+  if (ta == TTCB_S && tb == TTCB_S) return pick_kernel_ss(kernel, va, vb, variant);
+  if (ta == TTCB_D && tb == TTCB_D) return pick_kernel_dd(kernel, va, vb, variant);
+  if (ta == TTCB_C && tb == TTCB_C) return pick_kernel_cc(kernel, va, vb, variant);
+  if (ta == TTCB_Z && tb == TTCB_Z) return pick_kernel_zz(kernel, va, vb, variant);
+  if (ta == TTCB_S && tb == TTCB_D) return pick_kernel_sd(kernel, va, vb, variant);
+  if (ta == TTCB_D && tb == TTCB_S) return pick_kernel_ds(kernel, va, vb, variant);
+  if (ta == TTCB_C && tb == TTCB_Z) return pick_kernel_cz(kernel, va, vb, variant);
+  if (ta == TTCB_Z && tb == TTCB_C) return pick_kernel_zc(kernel, va, vb, variant);
+  return KernelRef();
+}
+}  // namespace ttcb
+
+static thread_local std::string g_last_error;
+
+static ttcb_status fail(ttcb_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+static ttcb_status cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return fail(TTCB_ERR_CUDA, m);
+}
+
+static int variant_of(const ttcb_plan* p) { return p->beta_nonzero ? 2 : (p->streaming ? 1 : 0); }
+
+// Kernels whose dynamic shared memory may exceed the 48 KB default get the opt-in once.
+static void allow_large_smem(const void* func) {
+  static std::mutex mu;
+  static const void* done[512];
+  static int ndone = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  for (int i = 0; i < ndone; ++i)
+    if (done[i] == func) return;
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaGetLastError();
+  if (ndone < 512) done[ndone++] = func;
+}
+
+static ttcb_status plan_finish_device(ttcb_plan* p) {
+  if (p->empty) return TTCB_OK;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  e = cudaMalloc(&p->dev_desc, p->host_desc.size());
+  if (e != cudaSuccess) {
+    p->dev_desc = nullptr;
+    cudaGetLastError();
+    return fail(TTCB_ERR_ALLOC, std::string("cudaMalloc of the plan descriptor failed: ") + cudaGetErrorString(e));
+  }
+  e = cudaMemcpy(p->dev_desc, p->host_desc.data(), p->host_desc.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy of the plan descriptor");
+
+  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, p->kernel, p->vecA, p->vecB, variant_of(p));
+  if (!k.func) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
+  if (p->smem_bytes > 48 * 1024) allow_large_smem(k.func);
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, p->smem_bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
+  int64_t work = 1;
+  if (p->kernel == TTCB_KERNEL_TILE) {
+    work = reinterpret_cast<const TileDesc*>(p->host_desc.data())->ntiles;
+  } else {
+    const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
+    work = (rd->nunits + (ttcb::kThreads / 32) - 1) / (ttcb::kThreads / 32);  // one warp per unit
+  }
+  int64_t resident = (int64_t)per_sm * sms;
+  int64_t blocks;
+  if (p->tuning.blocks > 0) {
+    blocks = std::min<int64_t>(p->tuning.blocks, work);
+  } else {
+    int64_t per = (work + resident - 1) / resident;  // work items per CTA, balanced
+    blocks = (work + per - 1) / per;
+  }
+  if (blocks < 1) blocks = 1;
+  p->blocks = (int)blocks;
+  return TTCB_OK;
+}
+
+extern "C" {
+
+ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const int64_t* size, const int64_t* lda,
+                             const int64_t* ldb, ttcb_dtype type_a, ttcb_dtype type_b, int beta_nonzero,
+                             const ttcb_tuning* tuning) {
+  if (!plan) return fail(TTCB_ERR_INVALID_ARG, "plan output pointer is NULL");
+  *plan = nullptr;
+  if (rank < 1 || rank > TTCB_MAX_RANK)
+    return fail(TTCB_ERR_RANK, "rank must be in [1, " + std::to_string(TTCB_MAX_RANK) + "], got " + std::to_string(rank));
+  if (!perm || !size) return fail(TTCB_ERR_INVALID_ARG, "perm and size must not be NULL");
+  ttcb_plan* p = new (std::nothrow) ttcb_plan();
+  if (!p) return fail(TTCB_ERR_ALLOC, "host allocation of the plan failed");
+  p->rank = rank;
+  for (int i = 0; i < rank; ++i) {
+    p->perm[i] = perm[i];
+    p->size[i] = size[i];
+  }
+  // perm must be checked before ldb's default uses it
+  {
+    bool seen[TTCB_MAX_RANK] = {false};
+    for (int j = 0; j < rank; ++j) {
+      if (perm[j] < 0 || perm[j] >= rank || seen[perm[j]]) {
+        delete p;
+        return fail(TTCB_ERR_BAD_PERM, "permutation is invalid");
+      }
+      seen[perm[j]] = true;
+    }
+  }
+  for (int i = 0; i < rank; ++i) p->lda[i] = lda ? lda[i] : size[i];
+  for (int j = 0; j < rank; ++j) p->ldb[j] = ldb ? ldb[j] : size[perm[j]];
+  p->ta = type_a;
+  p->tb = type_b;
+  p->beta_nonzero = beta_nonzero ? 1 : 0;
+  if (tuning) p->tuning = *tuning;
+  std::string err;
+  ttcb_status s = plan_build_host(p, err);
+  if (s != TTCB_OK) {
+    delete p;
+    return fail(s, err);
+  }
+  s = plan_finish_device(p);
+  if (s != TTCB_OK) {
+    if (p->dev_desc) cudaFree(p->dev_desc);
+    delete p;
+    return s;
+  }
+  *plan = p;
+  return TTCB_OK;
+}
+
+void ttcb_plan_destroy(ttcb_plan* plan) {
+  if (!plan) return;
+  if (plan->dev_desc) cudaFree(plan->dev_desc);
+  delete plan;
+}
+
+ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
+                           ttcb_stream_t stream) {
+  if (!p) return fail(TTCB_ERR_INVALID_ARG, "plan is NULL");
+  if (p->empty) return TTCB_OK;
+  if (!A || !B || !alpha) return fail(TTCB_ERR_INVALID_ARG, "A, B and alpha must not be NULL");
+  if (p->beta_nonzero && !beta) return fail(TTCB_ERR_BETA, "plan was created for beta != 0 but beta is NULL");
+  const int EA = dtype_bytes(p->ta), EB = dtype_bytes(p->tb);
+  const int natA = (p->ta == TTCB_C) ? 8 : EA, natB = (p->tb == TTCB_C) ? 8 : EB;
+  if ((uintptr_t)A % natA || (uintptr_t)B % natB)
+    return fail(TTCB_ERR_ALIGN, "A or B is not aligned to its element size");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != p->device)
+    return fail(TTCB_ERR_INVALID_ARG, "plan was created on device " + std::to_string(p->device) +
+                                          " but the current device is " + std::to_string(dev));
+  int va = p->vecA, vb = p->vecB;
+  if (p->kernel == TTCB_KERNEL_ROW) {
+    const int bytes = va * std::max(EA, EB);
+    if ((uintptr_t)A % (va * EA) || (uintptr_t)B % (vb * EB) || bytes > 16) va = vb = 1;
+  } else {
+    if ((uintptr_t)A % (va * EA)) va = 1;
+    if ((uintptr_t)B % (vb * EB)) vb = 1;
+  }
+  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, p->kernel, va, vb, variant_of(p));
+  if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
+  if (p->smem_bytes > 48 * 1024) allow_large_smem(k.func);
+  e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), p->blocks);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return TTCB_OK;
+}
+
+size_t ttcb_plan_describe(const ttcb_plan* plan, char* buf, size_t len) {
+  if (!plan) return 0;
+  std::string s = plan_describe_json(plan);
+  if (buf && len > 0) {
+    size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return s.size() + 1;
+}
+
+int64_t ttcb_plan_bytes(const ttcb_plan* p) {
+  if (!p) return 0;
+  return p->N * (dtype_bytes(p->ta) + (p->beta_nonzero ? 2 : 1) * dtype_bytes(p->tb));
+}
+
+const char* ttcb_last_error(void) { return g_last_error.c_str(); }
+
+void ttcb_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+void ttcb_version(int* major, int* minor, int* patch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (patch) *patch = 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Test hooks (declared in testing.h, not part of the public header).
+int ttcb_test_fuse(int rank, const int* perm, const int64_t* n, const int64_t* sA, const int64_t* sB, int* out_rank,
+                   int* out_perm, int64_t* out_n, int64_t* out_sA, int64_t* out_sB) {
+  if (rank < 1 || rank > TTCB_MAX_RANK) return -1;
+  FusedProblem f;
+  fuse_problem(rank, perm, n, sA, sB, f);
+  *out_rank = f.rank;
+  for (int i = 0; i < f.rank; ++i) {
+    out_perm[i] = f.perm[i];
+    out_n[i] = f.n[i];
+    out_sA[i] = f.sA[i];
+    out_sB[i] = f.sB[i];
+  }
+  return 0;
+}
+
+// Builds the host part of a plan (no CUDA calls) and returns its JSON description.
+int ttcb_test_plan_host(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                        int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len) {
+  ttcb_plan p;
+  p.rank = rank;
+  if (rank < 1 || rank > TTCB_MAX_RANK) return TTCB_ERR_RANK;
+  for (int i = 0; i < rank; ++i) {
+    p.perm[i] = perm[i];
+    p.size[i] = size[i];
+  }
+  for (int j = 0; j < rank; ++j)
+    if (perm[j] < 0 || perm[j] >= rank) return TTCB_ERR_BAD_PERM;
+  for (int i = 0; i < rank; ++i) p.lda[i] = lda ? lda[i] : size[i];
+  for (int j = 0; j < rank; ++j) p.ldb[j] = ldb ? ldb[j] : size[perm[j]];
+  p.ta = (ttcb_dtype)type_a;
+  p.tb = (ttcb_dtype)type_b;
+  p.beta_nonzero = beta_nonzero;
+  if (tuning) p.tuning = *tuning;
+  std::string err;
+  ttcb_status s = plan_build_host(&p, err);
+  if (s != TTCB_OK) {
+    g_last_error = err;
+    return s;
+  }
+  std::string js = plan_describe_json(&p);
+  if (buf && len) {
+    size_t n = std::min(len - 1, js.size());
+    std::memcpy(buf, js.data(), n);
+    buf[n] = 0;
+  }
+  return 0;
+}
+
+// Host-side copy of a plan's descriptor tables (for CPU checks of the tile tables).
+size_t ttcb_test_plan_desc(const ttcb_plan* p, void* buf, size_t len) {
+  if (!p) return 0;
+  if (buf && len >= p->host_desc.size()) std::memcpy(buf, p->host_desc.data(), p->host_desc.size());
+  return p->host_desc.size();
+}
+
+// Host-only plan build that returns the descriptor bytes (tile or row tables) and the kernel kind.
+size_t ttcb_test_plan_host_desc(int rank, const int* perm, const int64_t* size, const int64_t* lda,
+                                const int64_t* ldb, int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning,
+                                int* kernel, void* buf, size_t len) {
+  ttcb_plan p;
+  if (rank < 1 || rank > TTCB_MAX_RANK) return 0;
+  p.rank = rank;
+  for (int i = 0; i < rank; ++i) {
+    p.perm[i] = perm[i];
+    p.size[i] = size[i];
+  }
+  for (int j = 0; j < rank; ++j)
+    if (perm[j] < 0 || perm[j] >= rank) return 0;
+  for (int i = 0; i < rank; ++i) p.lda[i] = lda ? lda[i] : size[i];
+  for (int j = 0; j < rank; ++j) p.ldb[j] = ldb ? ldb[j] : size[perm[j]];
+  p.ta = (ttcb_dtype)type_a;
+  p.tb = (ttcb_dtype)type_b;
+  p.beta_nonzero = beta_nonzero;
+  if (tuning) p.tuning = *tuning;
+  std::string err;
+  if (plan_build_host(&p, err) != TTCB_OK) {
+    g_last_error = err;
+    return 0;
+  }
+  if (kernel) *kernel = p.kernel;
+  if (buf && len >= p.host_desc.size()) std::memcpy(buf, p.host_desc.data(), p.host_desc.size());
+  return p.host_desc.size();
+}
+
+// Layout of the descriptor structs, so host-side checkers can parse them.
+void ttcb_test_desc_layout(int64_t* out) {
+  out[0] = sizeof(TileDesc);
+  out[1] = offsetof(TileDesc, divLA);
+  out[2] = offsetof(TileDesc, g);
+  out[3] = sizeof(GridDimDesc);
+  out[4] = offsetof(TileDesc, bd);
+  out[5] = sizeof(BlockedDesc);
+  out[6] = sizeof(RowDesc);
+  out[7] = offsetof(RowDesc, div);
+  out[8] = offsetof(RowDesc, sA);
+  out[9] = offsetof(RowDesc, sB);
+  out[10] = sizeof(FastDiv);
+}
+
+uint32_t ttcb_test_fastdiv(uint32_t n, uint32_t d) {
+  FastDiv f = make_fastdiv(d);
+  return fdiv(n, f);
+}
+
+}  // extern "C"

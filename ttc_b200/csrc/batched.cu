@@ -1,0 +1,271 @@
+// C ABI of batched mode: one persistent launch (optionally replayed from a captured CUDA graph)
+// for many independent transpositions, each with the schedule of its own plan.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ttcb200.h"
+#include "batch_kernels.cuh"
+#include "launch.h"
+#include "plan.h"
+
+namespace ttcb {
+BatchKernelRef pick_batch_ss(int);
+BatchKernelRef pick_batch_dd(int);
+BatchKernelRef pick_batch_cc(int);
+BatchKernelRef pick_batch_zz(int);
+BatchKernelRef pick_batch_sd(int);
+BatchKernelRef pick_batch_ds(int);
+BatchKernelRef pick_batch_cz(int);
+BatchKernelRef pick_batch_zc(int);
+
+BatchKernelRef pick_batch_kernel(ttcb_dtype ta, ttcb_dtype tb, int variant) {
+  if (ta == TTCB_S && tb == TTCB_S) return pick_batch_ss(variant);
+  if (ta == TTCB_D && tb == TTCB_D) return pick_batch_dd(variant);
+  if (ta == TTCB_C && tb == TTCB_C) return pick_batch_cc(variant);
+  if (ta == TTCB_Z && tb == TTCB_Z) return pick_batch_zz(variant);
+  if (ta == TTCB_S && tb == TTCB_D) return pick_batch_sd(variant);
+  if (ta == TTCB_D && tb == TTCB_S) return pick_batch_ds(variant);
+  if (ta == TTCB_C && tb == TTCB_Z) return pick_batch_cz(variant);
+  if (ta == TTCB_Z && tb == TTCB_C) return pick_batch_zc(variant);
+  return BatchKernelRef();
+}
+}  // namespace ttcb
+
+struct ttcb_batch {
+  int count = 0;
+  ttcb_dtype ta = TTCB_S, tb = TTCB_S;
+  int beta_nonzero = 0;
+  bool streaming = false;
+  int device = 0;
+  unsigned char alpha[16] = {0};
+  unsigned char beta[16] = {0};
+  int64_t bytes = 0;
+  unsigned long long total = 0;
+  int blocks = 0;
+  int smem = 0;
+  void* d_probs = nullptr;
+  int64_t* d_prefix = nullptr;
+  unsigned char* d_desc = nullptr;
+  unsigned long long* d_counter = nullptr;  // [0] next item, [1] status word (as int)
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaStream_t capture_stream = nullptr;
+};
+
+// The thread-local last-error message lives in abi.cu.
+extern "C" void ttcb_internal_set_error(const char* msg);
+static ttcb_status bfail(ttcb_status s, const std::string& msg) {
+  ttcb_internal_set_error(msg.c_str());
+  return s;
+}
+static ttcb_status bcuda(cudaError_t e, const char* what) {
+  return bfail(TTCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+static void batch_free(ttcb_batch* b) {
+  if (!b) return;
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+  if (b->d_probs) cudaFree(b->d_probs);
+  if (b->d_prefix) cudaFree(b->d_prefix);
+  if (b->d_desc) cudaFree(b->d_desc);
+  if (b->d_counter) cudaFree(b->d_counter);
+  delete b;
+}
+
+static int batch_variant(const ttcb_batch* b) { return b->beta_nonzero ? 2 : (b->streaming ? 1 : 0); }
+
+extern "C" {
+
+ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* const* plans, const void* const* A,
+                              void* const* B, const void* alpha, const void* beta, int blocks) {
+  if (!out) return bfail(TTCB_ERR_INVALID_ARG, "batch output pointer is NULL");
+  *out = nullptr;
+  if (count < 1 || !plans || !A || !B || !alpha) return bfail(TTCB_ERR_INVALID_ARG, "empty batch or NULL argument");
+  const ttcb_plan* p0 = plans[0];
+  if (!p0) return bfail(TTCB_ERR_INVALID_ARG, "plan 0 is NULL");
+  if (p0->beta_nonzero && !beta) return bfail(TTCB_ERR_BETA, "plans were created for beta != 0 but beta is NULL");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return bcuda(e, "cudaGetDevice");
+  const int EA = dtype_bytes(p0->ta), EB = dtype_bytes(p0->tb);
+
+  ttcb_batch* b = new (std::nothrow) ttcb_batch();
+  if (!b) return bfail(TTCB_ERR_ALLOC, "host allocation of the batch failed");
+  b->count = count;
+  b->ta = p0->ta;
+  b->tb = p0->tb;
+  b->beta_nonzero = p0->beta_nonzero;
+  b->streaming = p0->streaming;
+  b->device = dev;
+  std::memcpy(b->alpha, alpha, EA);
+  if (p0->beta_nonzero) std::memcpy(b->beta, beta, EB);
+
+  // descriptors back to back, 16-byte aligned
+  std::vector<int64_t> desc_off(count, -1);
+  int64_t desc_bytes = 0;
+  for (int i = 0; i < count; ++i) {
+    const ttcb_plan* p = plans[i];
+    if (!p) {
+      batch_free(b);
+      return bfail(TTCB_ERR_INVALID_ARG, "plan " + std::to_string(i) + " is NULL");
+    }
+    if (p->ta != b->ta || p->tb != b->tb || p->beta_nonzero != b->beta_nonzero) {
+      batch_free(b);
+      return bfail(TTCB_ERR_INVALID_ARG, "all plans of a batch need the same types and beta flag");
+    }
+    if (p->device != dev && !p->empty) {
+      batch_free(b);
+      return bfail(TTCB_ERR_INVALID_ARG, "plan " + std::to_string(i) + " belongs to another device");
+    }
+    if (!p->empty) {
+      desc_off[i] = desc_bytes;
+      desc_bytes += (p->host_desc.size() + 15) & ~size_t(15);
+    }
+  }
+  std::vector<unsigned char> hdesc(std::max<int64_t>(desc_bytes, 16), 0);
+  std::vector<ttcb::BatchProblem> hp(count);
+  std::vector<int64_t> prefix(count + 1, 0);
+  int max_slots_bytes = 0;
+  for (int i = 0; i < count; ++i) {
+    const ttcb_plan* p = plans[i];
+    ttcb::BatchProblem& q = hp[i];
+    std::memset(&q, 0, sizeof(q));
+    int64_t items = 0;
+    if (!p->empty) {
+      if (!A[i] || !B[i]) {
+        batch_free(b);
+        return bfail(TTCB_ERR_INVALID_ARG, "A or B of problem " + std::to_string(i) + " is NULL");
+      }
+      std::memcpy(hdesc.data() + desc_off[i], p->host_desc.data(), p->host_desc.size());
+      q.A = A[i];
+      q.B = B[i];
+      q.kind = p->kernel;
+      q.va = p->vecA;
+      q.vb = p->vecB;
+      if (p->kernel == TTCB_KERNEL_ROW) {
+        if ((uintptr_t)A[i] % (q.va * EA) || (uintptr_t)B[i] % (q.vb * EB)) q.va = q.vb = 1;
+        const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
+        items = (rd->nunits + 7) / 8;
+      } else {
+        if ((uintptr_t)A[i] % (q.va * EA)) q.va = 1;
+        if ((uintptr_t)B[i] % (q.vb * EB)) q.vb = 1;
+        const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+        items = td->ntiles;
+        max_slots_bytes = std::max<int>(max_slots_bytes, (int)ttcb::tile_slots_bytes(td->phys_size, EA));
+      }
+      b->bytes += ttcb_plan_bytes(p);
+    }
+    prefix[i + 1] = prefix[i] + items;
+  }
+  b->total = (unsigned long long)prefix[count];
+  b->smem = max_slots_bytes;
+
+  // device copies
+  if ((e = cudaMalloc(&b->d_desc, hdesc.size())) != cudaSuccess ||
+      (e = cudaMalloc(&b->d_probs, sizeof(ttcb::BatchProblem) * count)) != cudaSuccess ||
+      (e = cudaMalloc(&b->d_prefix, sizeof(int64_t) * (count + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&b->d_counter, 2 * sizeof(unsigned long long))) != cudaSuccess) {
+    cudaGetLastError();
+    batch_free(b);
+    return bfail(TTCB_ERR_ALLOC, std::string("cudaMalloc for the batch failed: ") + cudaGetErrorString(e));
+  }
+  for (int i = 0; i < count; ++i)
+    if (desc_off[i] >= 0) hp[i].desc = b->d_desc + desc_off[i];
+  if ((e = cudaMemcpy(b->d_desc, hdesc.data(), hdesc.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->d_probs, hp.data(), sizeof(ttcb::BatchProblem) * count, cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (e = cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (e = cudaMemset(b->d_counter, 0, 2 * sizeof(unsigned long long))) != cudaSuccess) {
+    batch_free(b);
+    return bcuda(e, "batch descriptor upload");
+  }
+
+  ttcb::BatchKernelRef k = ttcb::pick_batch_kernel(b->ta, b->tb, batch_variant(b));
+  if (!k.func) {
+    batch_free(b);
+    return bfail(TTCB_ERR_DTYPE, "no batched kernel for this type pair");
+  }
+  if (b->smem > 48 * 1024) cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, b->smem);
+  if (e != cudaSuccess || per_sm < 1) {
+    batch_free(b);
+    return e != cudaSuccess ? bcuda(e, "occupancy query") : bfail(TTCB_ERR_UNSUPPORTED, "batch tile too large");
+  }
+  int64_t resident = (int64_t)per_sm * sms;
+  int64_t nb = blocks > 0 ? blocks : resident;
+  nb = std::min<int64_t>(nb, std::max<unsigned long long>(b->total, 1ull));
+  b->blocks = (int)std::max<int64_t>(nb, 1);
+  *out = b;
+  return TTCB_OK;
+}
+
+static ttcb_status batch_enqueue(ttcb_batch* b, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return bcuda(e, "counter reset");
+  if (b->total == 0) return TTCB_OK;
+  ttcb::BatchKernelRef k = ttcb::pick_batch_kernel(b->ta, b->tb, batch_variant(b));
+  e = k.fn(b->d_probs, b->d_prefix, b->count, b->total, b->d_counter,
+           reinterpret_cast<int*>(b->d_counter + 1), b->alpha, b->beta, b->blocks, b->smem, s);
+  if (e != cudaSuccess) return bcuda(e, "batched kernel launch");
+  return TTCB_OK;
+}
+
+ttcb_status ttcb_batch_launch(ttcb_batch* b, ttcb_stream_t stream) {
+  if (!b) return bfail(TTCB_ERR_INVALID_ARG, "batch is NULL");
+  return batch_enqueue(b, reinterpret_cast<cudaStream_t>(stream));
+}
+
+ttcb_status ttcb_batch_graph_launch(ttcb_batch* b, ttcb_stream_t stream) {
+  if (!b) return bfail(TTCB_ERR_INVALID_ARG, "batch is NULL");
+  cudaError_t e;
+  if (!b->graph_exec) {
+    // capture once on a private stream (the legacy default stream cannot be captured)
+    if ((e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return bcuda(e, "cudaStreamCreate");
+    if ((e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return bcuda(e, "cudaStreamBeginCapture");
+    ttcb_status st = batch_enqueue(b, b->capture_stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->capture_stream, &g);
+    if (st != TTCB_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return bcuda(e, "cudaStreamEndCapture");
+    b->graph = g;
+    if ((e = cudaGraphInstantiate(&b->graph_exec, g, 0)) != cudaSuccess) {
+      b->graph_exec = nullptr;
+      return bcuda(e, "cudaGraphInstantiate");
+    }
+  }
+  if ((e = cudaGraphLaunch(b->graph_exec, reinterpret_cast<cudaStream_t>(stream))) != cudaSuccess)
+    return bcuda(e, "cudaGraphLaunch");
+  return TTCB_OK;
+}
+
+ttcb_status ttcb_batch_status(ttcb_batch* b, ttcb_stream_t stream) {
+  if (!b) return bfail(TTCB_ERR_INVALID_ARG, "batch is NULL");
+  int st = 0;
+  cudaError_t e = cudaMemcpyAsync(&st, b->d_counter + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                  reinterpret_cast<cudaStream_t>(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return bcuda(e, "batch status read");
+  if (st != 0) return bfail(TTCB_ERR_INVALID_ARG, "batched kernel reported status " + std::to_string(st));
+  return TTCB_OK;
+}
+
+int64_t ttcb_batch_bytes(const ttcb_batch* b) { return b ? b->bytes : 0; }
+
+void ttcb_batch_destroy(ttcb_batch* b) { batch_free(b); }
+
+}  // extern "C"

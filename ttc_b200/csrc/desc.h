@@ -1,0 +1,71 @@
+// Device descriptors built once per plan by the host planner (plan.cpp) and read by the kernels.
+//
+// A plan is executed by one of two kernels:
+//
+//  * tile kernel: the index space is cut into tiles of P elements. A tile is a product set over a
+//    subset T of the (fused) dimensions: the leading A dimensions (A's contiguous "run") and the
+//    leading B dimensions (B's run), each either full or blocked. Inside a tile, elements are
+//    numbered in A order (p) and in B order (q). The load phase walks p (contiguous runs of LA
+//    elements in A, segment bases in segA[]), scales by alpha and scatters into shared memory at
+//    slot perm_tab[p]; the store phase walks q (runs of LB elements in B, bases in segB[]) and
+//    writes B. The remaining dimensions, and the block index of blocked dimensions, form the tile
+//    grid, rasterised in the plan's loop order. This generalises TTC's 32x32 plane tiles
+//    (CUDAtranspose.py:114-165, 289-388) to runs that span several dimensions.
+//
+//  * row kernel: when A's and B's stride-1 dimension is the same one and long (TTC's perm[0]==0
+//    path, CUDAtranspose.py:179-243, and its identity copy, :781-799), rows are copied directly,
+//    one warp per (row, chunk) unit, without staging.
+#pragma once
+#include <cstdint>
+#include "common.cuh"
+
+struct GridDimDesc {
+  FastDiv div;      // number of grid steps along this dimension
+  int64_t strideA;  // A element offset of one grid step (block extent * A stride)
+  int64_t strideB;  // B element offset of one grid step
+  int64_t n;        // full extent of the dimension
+  int32_t e;        // tile extent (1 for dimensions outside the tile)
+  int32_t blocked;  // index into TileDesc::bd for a blocked tile dimension, else -1
+};
+
+struct BlockedDesc {
+  FastDiv tsA;  // stride of this dimension in the tile's A-order numbering p
+  FastDiv tsB;  // stride in the tile's B-order numbering q
+  FastDiv ext;  // tile extent e of the dimension
+};
+
+struct TileDesc {
+  int32_t P;          // elements per tile
+  int32_t LA, LB;     // contiguous run lengths (elements) in A and in B
+  int32_t nsegA;      // P / LA
+  int32_t nsegB;      // P / LB
+  int32_t pshift;     // shared-memory slot of q: q + (q >> pshift) * pad
+  int32_t pad;
+  int32_t phys_size;  // shared-memory slots including padding
+  int32_t ngrid;      // grid dimensions, fastest first
+  int32_t nblocked;   // blocked tile dimensions (0..2)
+  int32_t ntiles;
+  int32_t off_segA;   // byte offsets of the tables, relative to the start of the descriptor
+  int32_t off_segB;
+  int32_t off_perm;
+  int32_t smem_bytes; // dynamic shared memory the kernel needs
+  int32_t pad_[1];
+  FastDiv divLA, divLB;
+  GridDimDesc g[TTCB_MAXR];
+  BlockedDesc bd[2];
+  // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
+};
+
+struct RowDesc {
+  int64_t w;          // row length in elements (stride 1 in both A and B)
+  int32_t chunk;      // elements per work unit
+  int32_t nchunk;     // units per row
+  int32_t nd;         // number of row dimensions
+  int32_t nunits;     // rows * nchunk
+  FastDiv divChunk;   // divisor nchunk
+  FastDiv div[TTCB_MAXR];
+  int64_t sA[TTCB_MAXR];
+  int64_t sB[TTCB_MAXR];
+};
+
+enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };

@@ -1,0 +1,639 @@
+// Host planner: validation, index fusion, kernel choice, tile shape search, descriptor tables.
+//
+// Reference behaviour that is restated here (TTC, file:line inside the TTC project):
+//   validation            ttc.py:733-768 (lda/ldb >= size, perm is a permutation)
+//   strides from lda/ldb  CUDAtranspose.py:543-556, GPUreference.py:217-230
+//                         (stride of A-dim i = prod_{k<i} lda[k], B-dim j = prod_{k<j} ldb[k])
+//   index fusion          ttc_util.py:214-276 (merge A-dims i,i+1 that are also adjacent in B and
+//                         unpadded); extent-1 dimensions are dropped as well, which changes no
+//                         result
+//   path classification   CUDAtranspose.py:34-42 (identity / perm[0]==0 / general)
+// The blocking/loop-order search of GPUtransposeGenerator.py:165-285 is replaced by a cost model
+// over multi-dimensional tiles (below) whose knobs the autotuner searches.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+int dtype_bytes(ttcb_dtype t) {
+  switch (t) {
+    case TTCB_S: return 4;
+    case TTCB_D: return 8;
+    case TTCB_C: return 8;
+    case TTCB_Z: return 16;
+  }
+  return 0;
+}
+
+static bool dtype_complex(ttcb_dtype t) { return t == TTCB_C || t == TTCB_Z; }
+
+static bool mul_ok(int64_t a, int64_t b, int64_t* out) { return !__builtin_mul_overflow(a, b, out); }
+
+static int64_t gcd64(int64_t a, int64_t b) {
+  if (a < 0) a = -a;
+  if (b < 0) b = -b;
+  while (b) {
+    int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// ------------------------------------------------------------------------------------------------
+void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA, const int64_t* sB,
+                  FusedProblem& out) {
+  struct Grp {
+    int64_t n, sA, sB;
+    int id;
+  };
+  std::vector<Grp> a;      // groups in A order
+  std::vector<int> border; // group ids in B order
+  for (int i = 0; i < rank; ++i)
+    if (n[i] != 1) a.push_back({n[i], sA[i], sB[i], i});
+  for (int j = 0; j < rank; ++j)
+    if (n[perm[j]] != 1) border.push_back(perm[j]);
+
+  bool changed = true;
+  while (changed) {
+    changed = false;
+    for (size_t k = 0; k + 1 < a.size(); ++k) {
+      const Grp& g = a[k];
+      const Grp& h = a[k + 1];
+      size_t pg = std::find(border.begin(), border.end(), g.id) - border.begin();
+      if (pg + 1 < border.size() && border[pg + 1] == h.id && h.sA == g.sA * g.n && h.sB == g.sB * g.n) {
+        a[k].n *= h.n;
+        border.erase(border.begin() + pg + 1);
+        a.erase(a.begin() + k + 1);
+        changed = true;
+        break;
+      }
+    }
+  }
+  out = FusedProblem();
+  if (a.empty()) {
+    out.rank = 1;
+    out.perm[0] = 0;
+    out.n[0] = 1;
+    out.sA[0] = 1;
+    out.sB[0] = 1;
+    return;
+  }
+  out.rank = (int)a.size();
+  for (int i = 0; i < out.rank; ++i) {
+    out.n[i] = a[i].n;
+    out.sA[i] = a[i].sA;
+    out.sB[i] = a[i].sB;
+  }
+  for (int j = 0; j < out.rank; ++j) {
+    int id = border[j];
+    for (int i = 0; i < out.rank; ++i)
+      if (a[i].id == id) out.perm[j] = i;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Cost model. Units: bytes of DRAM traffic (including wasted sector bytes) per element, plus a
+// fixed per-tile overhead expressed in the same unit.
+static double run_eff(double run_bytes, int64_t align_bytes) {
+  if (run_bytes <= 0) return 1e-3;
+  int64_t a = std::max<int64_t>(4, std::min<int64_t>(align_bytes, 32));
+  double sectors = 0;
+  int cnt = 0;
+  for (int64_t o = 0; o < 32; o += a) {
+    sectors += std::ceil((o + run_bytes) / 32.0);
+    ++cnt;
+  }
+  sectors /= cnt;
+  double eff = run_bytes / (32.0 * sectors);
+  if (run_bytes < 128) eff *= 0.75 + 0.25 * run_bytes / 128.0;  // short DRAM bursts
+  return eff;
+}
+
+struct TileCand {
+  int64_t ext[TTCB_MAXR];  // 0 = not in tile
+  int64_t P = 0;
+  int64_t LA = 1, LB = 1;
+  int64_t galA = 0, galB = 0;  // gcd of segment/grid offsets (elements); 0 = none
+  int vecA = 1, vecB = 1;
+  double cost = 1e30;
+};
+
+static void tile_orders(const FusedProblem& f, const int64_t* ext, std::vector<int>& aord, std::vector<int>& bord) {
+  aord.clear();
+  bord.clear();
+  for (int i = 0; i < f.rank; ++i)
+    if (ext[i] > 0) aord.push_back(i);
+  for (int j = 0; j < f.rank; ++j)
+    if (ext[f.perm[j]] > 0) bord.push_back(f.perm[j]);
+}
+
+static int64_t run_len(const std::vector<int>& order, const int64_t* ext, const int64_t* n, const int64_t* s) {
+  int64_t L = 1, expect = 1;
+  for (int d : order) {
+    if (s[d] != expect) break;
+    L *= ext[d];
+    if (ext[d] < n[d]) break;
+    expect = s[d] * n[d];
+  }
+  return L;
+}
+
+static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& c) {
+  std::vector<int> aord, bord;
+  tile_orders(f, c.ext, aord, bord);
+  c.P = 1;
+  for (int d : aord) c.P *= c.ext[d];
+  c.LA = run_len(aord, c.ext, f.n, f.sA);
+  c.LB = run_len(bord, c.ext, f.n, f.sB);
+  // alignment of segment starts and grid steps
+  int64_t gA = 0, gB = 0;
+  {
+    // A: dims of the tile beyond the A run contribute to segment offsets
+    int64_t acc = 1;
+    bool in_run = true;
+    for (int d : aord) {
+      if (in_run && acc < c.LA) {
+        acc *= c.ext[d];
+        continue;
+      }
+      in_run = false;
+      if (c.ext[d] > 1) gA = gcd64(gA, f.sA[d]);
+    }
+    acc = 1;
+    in_run = true;
+    for (int d : bord) {
+      if (in_run && acc < c.LB) {
+        acc *= c.ext[d];
+        continue;
+      }
+      in_run = false;
+      if (c.ext[d] > 1) gB = gcd64(gB, f.sB[d]);
+    }
+    for (int d = 0; d < f.rank; ++d) {
+      int64_t e = c.ext[d] > 0 ? c.ext[d] : 1;
+      if (c.ext[d] > 0 && c.ext[d] == f.n[d]) continue;  // full tile dim: no grid steps
+      gA = gcd64(gA, e * f.sA[d]);
+      gB = gcd64(gB, e * f.sB[d]);
+    }
+  }
+  c.galA = gA;
+  c.galB = gB;
+  int VA = 16 / EA, VB = 16 / EB;
+  c.vecA = (VA > 1 && c.LA % VA == 0 && (gA == 0 || gA % VA == 0)) ? VA : 1;
+  c.vecB = (VB > 1 && c.LB % VB == 0 && (gB == 0 || gB % VB == 0)) ? VB : 1;
+  if (tu.vec == 1) c.vecA = c.vecB = 1;
+
+  int64_t alA = gA == 0 ? 128 : std::min<int64_t>(128, (gA * EA) & -(gA * EA));
+  int64_t alB = gB == 0 ? 128 : std::min<int64_t>(128, (gB * EB) & -(gB * EB));
+  double effA = run_eff((double)c.LA * EA, alA);
+  double effB = run_eff((double)c.LB * EB, alB);
+  double per_elem = EA / effA + (beta ? 2.0 : 1.0) * EB / effB;
+  if (c.vecA == 1 && EA < 16) per_elem += 0.15 * EA;  // more instructions per byte
+  if (c.vecB == 1 && EB < 16) per_elem += 0.15 * EB * (beta ? 2.0 : 1.0);
+
+  // average useful elements per tile (ragged last blocks waste a tile's fixed cost)
+  double fill = 1.0;
+  int64_t ntiles = 1;
+  for (int d = 0; d < f.rank; ++d) {
+    if (c.ext[d] == 0) {
+      ntiles *= f.n[d];
+    } else if (c.ext[d] < f.n[d]) {
+      int64_t nb = (f.n[d] + c.ext[d] - 1) / c.ext[d];
+      ntiles *= nb;
+      fill *= (double)f.n[d] / (double)(nb * c.ext[d]);
+    }
+  }
+  double tile_overhead = 3072.0;  // bytes-equivalent per tile
+  double cost = per_elem + tile_overhead / (c.P * fill);
+
+  // shared memory footprint and residency
+  int64_t nsegA = c.P / c.LA, nsegB = c.P / c.LB;
+  double smem = c.P * EA * 1.07 + 8.0 * (nsegA + nsegB) + 2.0 * c.P;
+  int ctas = (int)std::min(8.0, std::floor(227.0 * 1024 / (smem + 1024)));
+  if (ctas < 4) cost *= 1.0 + 0.08 * (4 - ctas);
+  // too few tiles to fill 148 SMs
+  double need = 148.0 * 4;
+  if ((double)ntiles < need) cost *= 1.0 + 0.5 * (need - ntiles) / need;
+  if (tu.run_bytes > 0) {
+    double r = std::log2(std::max(1.0, (double)c.LA * EA) / tu.run_bytes);
+    cost *= 1.0 + 0.25 * std::fabs(r);
+  }
+  c.cost = cost;
+}
+
+static void block_choices(int64_t n, int64_t prefix, int EA, std::vector<int64_t>& out) {
+  out.clear();
+  out.push_back(n);
+  static const int64_t base[] = {2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 24, 32, 48, 64, 96, 128, 192, 256, 512};
+  for (int64_t b : base)
+    if (b < n) out.push_back(b);
+  for (int64_t bytes : {128, 256, 512, 1024}) {
+    int64_t b = (bytes / EA + prefix - 1) / std::max<int64_t>(prefix, 1);
+    if (b >= 2 && b < n) out.push_back(b);
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+}
+
+static bool best_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& best) {
+  const int r = f.rank;
+  int64_t Pmax = tu.tile_elems > 0 ? tu.tile_elems : 16384 / EA;
+  Pmax = std::min<int64_t>(Pmax, 8192);
+  int64_t maxseg = 1024;
+  bool found = false;
+  std::vector<int64_t> chA, chB;
+  for (int kA = 1; kA <= r; ++kA) {
+    int64_t prefA = 1;
+    for (int i = 0; i < kA - 1; ++i) prefA *= f.n[i];
+    if (prefA > Pmax) break;
+    block_choices(f.n[kA - 1], prefA, EA, chA);
+    for (int64_t eA : chA) {
+      for (int kB = 1; kB <= r; ++kB) {
+        int64_t prefB = 1;
+        for (int j = 0; j < kB - 1; ++j) prefB *= f.n[f.perm[j]];
+        if (prefB > Pmax) break;
+        block_choices(f.n[f.perm[kB - 1]], prefB, EB, chB);
+        for (int64_t eB : chB) {
+          TileCand c;
+          for (int i = 0; i < TTCB_MAXR; ++i) c.ext[i] = 0;
+          bool ok = true;
+          for (int i = 0; i < kA - 1; ++i) c.ext[i] = f.n[i];
+          c.ext[kA - 1] = eA;
+          for (int j = 0; j < kB && ok; ++j) {
+            int d = f.perm[j];
+            int64_t want = (j == kB - 1) ? eB : f.n[d];
+            if (c.ext[d] == 0) {
+              c.ext[d] = want;
+            } else if (c.ext[d] != want) {
+              ok = false;
+            }
+          }
+          if (!ok) continue;
+          int64_t P = 1;
+          for (int i = 0; i < r; ++i)
+            if (c.ext[i] > 0) {
+              if (!mul_ok(P, c.ext[i], &P) || P > Pmax) {
+                ok = false;
+                break;
+              }
+            }
+          if (!ok || P < 1) continue;
+          int nblk = 0;
+          for (int i = 0; i < r; ++i)
+            if (c.ext[i] > 0 && c.ext[i] < f.n[i]) ++nblk;
+          if (nblk > 2) continue;
+          eval_tile(f, EA, EB, beta, tu, c);
+          if (c.P / c.LA > maxseg || c.P / c.LB > maxseg) continue;
+          if (!found || c.cost < best.cost - 1e-9 ||
+              (std::fabs(c.cost - best.cost) <= 1e-9 && std::min(c.LA, c.LB) > std::min(best.LA, best.LB))) {
+            best = c;
+            found = true;
+          }
+        }
+      }
+    }
+  }
+  return found;
+}
+
+// ------------------------------------------------------------------------------------------------
+static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
+  const FusedProblem& f = p->f;
+  std::vector<int> aord, bord;
+  tile_orders(f, c.ext, aord, bord);
+  // tile strides in A order / B order
+  int64_t tsA[TTCB_MAXR] = {0}, tsB[TTCB_MAXR] = {0};
+  {
+    int64_t acc = 1;
+    for (int d : aord) {
+      tsA[d] = acc;
+      acc *= c.ext[d];
+    }
+    acc = 1;
+    for (int d : bord) {
+      tsB[d] = acc;
+      acc *= c.ext[d];
+    }
+  }
+  const int64_t P = c.P;
+  // padding of the shared-memory slots: consecutive p (A run) are sigma apart in q
+  int pshift = 30, pad = 0;
+  {
+    int64_t sigma = tsB[aord[0]];
+    if (sigma >= 4) {
+      int k = __builtin_ctzll((unsigned long long)sigma);
+      if (k >= 2) {
+        pshift = std::min(k, 12);
+        pad = 1;
+      }
+    }
+  }
+  auto phys = [&](int64_t q) { return q + (pad ? (q >> pshift) : 0); };
+  int64_t phys_size = phys(P - 1) + 1;
+
+  int64_t nsegA = P / c.LA, nsegB = P / c.LB;
+  std::vector<int64_t> segA(nsegA), segB(nsegB);
+  std::vector<uint16_t> ptab(P);
+  for (int64_t pp = 0; pp < P; ++pp) {
+    int64_t rem = pp, offA = 0, q = 0;
+    for (int d : aord) {
+      int64_t cd = rem % c.ext[d];
+      rem /= c.ext[d];
+      offA += cd * f.sA[d];
+      q += cd * tsB[d];
+    }
+    ptab[pp] = (uint16_t)phys(q);
+    if (pp % c.LA == 0) segA[pp / c.LA] = offA;
+  }
+  for (int64_t s = 0; s < nsegB; ++s) {
+    int64_t rem = s * c.LB, offB = 0;
+    for (int d : bord) {
+      int64_t cd = rem % c.ext[d];
+      rem /= c.ext[d];
+      offB += cd * f.sB[d];
+    }
+    segB[s] = offB;
+  }
+
+  TileDesc td;
+  std::memset(&td, 0, sizeof(td));
+  td.P = (int32_t)P;
+  td.LA = (int32_t)c.LA;
+  td.LB = (int32_t)c.LB;
+  td.nsegA = (int32_t)nsegA;
+  td.nsegB = (int32_t)nsegB;
+  td.pshift = pshift;
+  td.pad = pad;
+  td.phys_size = (int32_t)phys_size;
+  td.divLA = make_fastdiv((uint32_t)c.LA);
+  td.divLB = make_fastdiv((uint32_t)c.LB);
+
+  // grid dimensions, fastest first, in the requested loop order
+  std::vector<int> gdims;
+  if (p->loop_order == 1) {
+    for (int j = 0; j < f.rank; ++j) gdims.push_back(f.perm[j]);
+  } else if (p->loop_order == 2) {
+    for (int i = f.rank - 1; i >= 0; --i) gdims.push_back(i);
+  } else {
+    for (int i = 0; i < f.rank; ++i) gdims.push_back(i);
+  }
+  int ng = 0, nb = 0;
+  int64_t ntiles = 1;
+  for (int d : gdims) {
+    if (c.ext[d] > 0 && c.ext[d] == f.n[d]) continue;
+    int64_t e = c.ext[d] > 0 ? c.ext[d] : 1;
+    int64_t cnt = (f.n[d] + e - 1) / e;
+    GridDimDesc& g = td.g[ng++];
+    g.div = make_fastdiv((uint32_t)cnt);
+    g.strideA = e * f.sA[d];
+    g.strideB = e * f.sB[d];
+    g.n = f.n[d];
+    g.e = (int32_t)e;
+    g.blocked = -1;
+    if (c.ext[d] > 0) {
+      g.blocked = nb;
+      BlockedDesc& b = td.bd[nb++];
+      b.tsA = make_fastdiv((uint32_t)tsA[d]);
+      b.tsB = make_fastdiv((uint32_t)tsB[d]);
+      b.ext = make_fastdiv((uint32_t)e);
+    }
+    ntiles *= cnt;
+  }
+  td.ngrid = ng;
+  td.nblocked = nb;
+  td.ntiles = (int32_t)ntiles;
+
+  auto al16 = [](int64_t x) { return (x + 15) & ~int64_t(15); };
+  int64_t off = al16(sizeof(TileDesc));
+  td.off_segA = (int32_t)off;
+  off = al16(off + 8 * nsegA);
+  td.off_segB = (int32_t)off;
+  off = al16(off + 8 * nsegB);
+  td.off_perm = (int32_t)off;
+  off = al16(off + 2 * P);
+  int64_t smem = al16(phys_size * EA) + 8 * nsegA + 8 * nsegB + al16(2 * P);
+  td.smem_bytes = (int32_t)smem;
+
+  p->host_desc.assign(off, 0);
+  std::memcpy(p->host_desc.data(), &td, sizeof(td));
+  std::memcpy(p->host_desc.data() + td.off_segA, segA.data(), 8 * nsegA);
+  std::memcpy(p->host_desc.data() + td.off_segB, segB.data(), 8 * nsegB);
+  std::memcpy(p->host_desc.data() + td.off_perm, ptab.data(), 2 * P);
+  p->smem_bytes = (int)smem;
+  p->vecA = c.vecA;
+  p->vecB = c.vecB;
+  p->est_cost = c.cost;
+}
+
+static ttcb_status build_row_desc(ttcb_plan* p, std::string& err) {
+  const FusedProblem& f = p->f;
+  const int EA = dtype_bytes(p->ta), EB = dtype_bytes(p->tb);
+  RowDesc rd;
+  std::memset(&rd, 0, sizeof(rd));
+  rd.w = f.n[0];
+  int V = 16 / std::max(EA, EB);
+  int64_t g = 0;
+  for (int i = 1; i < f.rank; ++i) {
+    g = gcd64(g, f.sA[i]);
+    g = gcd64(g, f.sB[i]);
+  }
+  if (V > 1 && !(g == 0 || g % V == 0)) V = 1;
+  if (p->tuning.vec == 1) V = 1;
+  const int64_t chunk_max = 32 * V * 8;
+  int64_t chunk = rd.w <= chunk_max ? rd.w : chunk_max;
+  int64_t nchunk = (rd.w + chunk - 1) / chunk;
+  int64_t rows = 1;
+  rd.nd = f.rank - 1;
+  for (int i = 1; i < f.rank; ++i) {
+    rows *= f.n[i];
+    rd.div[i - 1] = make_fastdiv((uint32_t)f.n[i]);
+    rd.sA[i - 1] = f.sA[i];
+    rd.sB[i - 1] = f.sB[i];
+    if (f.n[i] >= (int64_t(1) << 31)) {
+      err = "row dimension extent >= 2^31 is not supported";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+  }
+  int64_t units = rows * nchunk;
+  if (units >= (int64_t(1) << 31) || nchunk >= (int64_t(1) << 31)) {
+    err = "row copy: more than 2^31 work units";
+    return TTCB_ERR_UNSUPPORTED;
+  }
+  rd.chunk = (int32_t)chunk;
+  rd.nchunk = (int32_t)nchunk;
+  rd.nunits = (int32_t)units;
+  rd.divChunk = make_fastdiv((uint32_t)nchunk);
+  p->host_desc.assign(sizeof(RowDesc), 0);
+  std::memcpy(p->host_desc.data(), &rd, sizeof(rd));
+  p->smem_bytes = 0;
+  p->vecA = p->vecB = V;
+  double eff = run_eff((double)rd.w * std::max(EA, EB), (g == 0 ? 128 : std::min<int64_t>(128, (g * EA) & -(g * EA))));
+  p->est_cost = (EA + (p->beta_nonzero ? 2.0 : 1.0) * EB) / eff;
+  return TTCB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
+  const int r = p->rank;
+  if (r < 1 || r > TTCB_MAXR) {
+    err = "rank must be in [1, " + std::to_string(TTCB_MAXR) + "], got " + std::to_string(r);
+    return TTCB_ERR_RANK;
+  }
+  {
+    bool seen[TTCB_MAXR] = {false};
+    for (int j = 0; j < r; ++j) {
+      int d = p->perm[j];
+      if (d < 0 || d >= r || seen[d]) {
+        err = "permutation is invalid";
+        return TTCB_ERR_BAD_PERM;
+      }
+      seen[d] = true;
+    }
+  }
+  for (int i = 0; i < r; ++i) {
+    if (p->size[i] < 0) {
+      err = "size[" + std::to_string(i) + "] is negative";
+      return TTCB_ERR_INVALID_ARG;
+    }
+    if (p->lda[i] < p->size[i]) {
+      err = "the leading dimension of A for dim " + std::to_string(i) + " is smaller than allowed (it must be >= " +
+            std::to_string(p->size[i]) + ")";
+      return TTCB_ERR_BAD_LD;
+    }
+  }
+  for (int j = 0; j < r; ++j) {
+    if (p->ldb[j] < p->size[p->perm[j]]) {
+      err = "the leading dimension of B for dim " + std::to_string(j) + " is smaller than allowed (it must be >= " +
+            std::to_string(p->size[p->perm[j]]) + ")";
+      return TTCB_ERR_BAD_LD;
+    }
+  }
+  if ((int)p->ta < 0 || (int)p->ta > 3 || (int)p->tb < 0 || (int)p->tb > 3 ||
+      dtype_complex(p->ta) != dtype_complex(p->tb)) {
+    err = "unsupported data type pair (valid: s, d, c, z, sd, ds, cz, zc)";
+    return TTCB_ERR_DTYPE;
+  }
+  const int EA = dtype_bytes(p->ta), EB = dtype_bytes(p->tb);
+
+  // strides
+  int64_t sA[TTCB_MAXR], sB[TTCB_MAXR], sBpos[TTCB_MAXR];
+  sA[0] = 1;
+  sBpos[0] = 1;
+  for (int i = 1; i < r; ++i) {
+    if (!mul_ok(sA[i - 1], std::max<int64_t>(p->lda[i - 1], 1), &sA[i]) ||
+        !mul_ok(sBpos[i - 1], std::max<int64_t>(p->ldb[i - 1], 1), &sBpos[i])) {
+      err = "stride overflow";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+  }
+  for (int j = 0; j < r; ++j) sB[p->perm[j]] = sBpos[j];
+  int64_t N = 1;
+  for (int i = 0; i < r; ++i) {
+    if (!mul_ok(N, p->size[i], &N)) {
+      err = "element count overflow";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+  }
+  p->N = N;
+  p->empty = (N == 0);
+  p->streaming = (p->tuning.streaming == 1) || (p->tuning.streaming == 0 && !p->beta_nonzero);
+  if (p->beta_nonzero) p->streaming = false;
+  p->loop_order = p->tuning.loop_order;
+  if (p->empty) {
+    p->kernel = 0;
+    p->f.rank = 0;
+    return TTCB_OK;
+  }
+  fuse_problem(r, p->perm, p->size, sA, sB, p->f);
+  const FusedProblem& f = p->f;
+  for (int i = 0; i < f.rank; ++i)
+    if (f.n[i] >= (int64_t(1) << 31) && !(f.perm[0] == 0 && i == 0)) {
+      err = "a fused extent >= 2^31 outside the shared stride-1 dimension is not supported";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+
+  const bool beta = p->beta_nonzero != 0;
+  // kernel choice
+  bool row_possible = (f.perm[0] == 0 && f.sA[0] == 1 && f.sB[0] == 1);
+  TileCand best;
+  bool have_tile = false;
+  if (!(row_possible && f.n[0] >= (int64_t(1) << 31))) have_tile = best_tile(f, EA, EB, beta, p->tuning, best);
+  int kernel = 0;
+  if (p->tuning.kernel == TTCB_KERNEL_ROW) {
+    if (!row_possible) {
+      err = "row kernel requested but A and B do not share their stride-1 dimension";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+    kernel = TTCB_KERNEL_ROW;
+  } else if (p->tuning.kernel == TTCB_KERNEL_TILE) {
+    if (!have_tile) {
+      err = "no tile shape fits this problem";
+      return TTCB_ERR_UNSUPPORTED;
+    }
+    kernel = TTCB_KERNEL_TILE;
+  } else {
+    if (row_possible) {
+      double rb = (double)f.n[0] * std::max(EA, EB);
+      double row_cost = (EA + (beta ? 2.0 : 1.0) * EB) / run_eff(rb, 16);
+      kernel = (!have_tile || rb >= 512 || row_cost <= best.cost * 1.05) ? TTCB_KERNEL_ROW : TTCB_KERNEL_TILE;
+    } else {
+      if (!have_tile) {
+        err = "no tile shape fits this problem";
+        return TTCB_ERR_UNSUPPORTED;
+      }
+      kernel = TTCB_KERNEL_TILE;
+    }
+  }
+  p->kernel = kernel;
+  if (kernel == TTCB_KERNEL_ROW) return build_row_desc(p, err);
+  {
+    // tile counts must fit the kernels' 32-bit tile index
+    int64_t ntiles = 1;
+    for (int d = 0; d < f.rank; ++d) {
+      int64_t e = best.ext[d] > 0 ? best.ext[d] : 1;
+      if (best.ext[d] > 0 && best.ext[d] == f.n[d]) continue;
+      ntiles *= (f.n[d] + e - 1) / e;
+      if (ntiles >= (int64_t(1) << 31)) {
+        err = "more than 2^31 tiles";
+        return TTCB_ERR_UNSUPPORTED;
+      }
+    }
+  }
+  build_tile_desc(p, best, EA);
+  return TTCB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+std::string plan_describe_json(const ttcb_plan* p) {
+  static const char* names[] = {"s", "d", "c", "z"};
+  std::ostringstream o;
+  o << "{\"rank\":" << p->rank << ",\"dtypeA\":\"" << names[p->ta] << "\",\"dtypeB\":\"" << names[p->tb]
+    << "\",\"beta\":" << (p->beta_nonzero ? 1 : 0) << ",\"elements\":" << p->N;
+  o << ",\"fused\":{\"rank\":" << p->f.rank << ",\"perm\":[";
+  for (int i = 0; i < p->f.rank; ++i) o << (i ? "," : "") << p->f.perm[i];
+  o << "],\"size\":[";
+  for (int i = 0; i < p->f.rank; ++i) o << (i ? "," : "") << p->f.n[i];
+  o << "],\"strideA\":[";
+  for (int i = 0; i < p->f.rank; ++i) o << (i ? "," : "") << p->f.sA[i];
+  o << "],\"strideB\":[";
+  for (int i = 0; i < p->f.rank; ++i) o << (i ? "," : "") << p->f.sB[i];
+  o << "]}";
+  o << ",\"kernel\":\"" << (p->kernel == TTCB_KERNEL_TILE ? "tile" : p->kernel == TTCB_KERNEL_ROW ? "row" : "none")
+    << "\",\"vecA\":" << p->vecA << ",\"vecB\":" << p->vecB << ",\"blocks\":" << p->blocks
+    << ",\"streaming\":" << (p->streaming ? 1 : 0) << ",\"loop_order\":" << p->loop_order
+    << ",\"smem\":" << p->smem_bytes << ",\"est_cost\":" << p->est_cost;
+  if (p->kernel == TTCB_KERNEL_TILE && !p->host_desc.empty()) {
+    const TileDesc* t = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    o << ",\"tile\":{\"P\":" << t->P << ",\"LA\":" << t->LA << ",\"LB\":" << t->LB << ",\"ntiles\":" << t->ntiles
+      << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
+      << ",\"pshift\":" << t->pshift << "}";
+  } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {
+    const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
+    o << ",\"row\":{\"w\":" << rd->w << ",\"chunk\":" << rd->chunk << ",\"units\":" << rd->nunits << "}";
+  }
+  o << "}";
+  return o.str();
+}

@@ -1,0 +1,19 @@
+// Test hooks exported by libttcb200.so for CPU-side unit tests. They are not part of the public
+// ABI (include/ttcb200.h) and make no CUDA calls.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include "../../include/ttcb200.h"
+
+extern "C" {
+int ttcb_test_fuse(int rank, const int* perm, const int64_t* n, const int64_t* sA, const int64_t* sB, int* out_rank,
+                   int* out_perm, int64_t* out_n, int64_t* out_sA, int64_t* out_sB);
+int ttcb_test_plan_host(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                        int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len);
+size_t ttcb_test_plan_desc(const ttcb_plan* p, void* buf, size_t len);
+uint32_t ttcb_test_fastdiv(uint32_t n, uint32_t d);
+size_t ttcb_test_plan_host_desc(int rank, const int* perm, const int64_t* size, const int64_t* lda,
+                                const int64_t* ldb, int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning,
+                                int* kernel, void* buf, size_t len);
+void ttcb_test_desc_layout(int64_t* out);
+}
