@@ -66,7 +66,9 @@ typedef struct {
   int32_t blocks;        /* CTAs launched (persistent grid); 0 = all tiles / occupancy bound  */
   int32_t loop_order;    /* 0 = A-major raster of the tile grid, 1 = B-major, 2 = reverse A   */
   int32_t streaming;     /* 0 = default (streaming stores when beta == 0), 1 = on, -1 = off     */
-  int32_t reserved[9];
+  int32_t tile_variant;  /* tile kernel: 0 auto, 1 table-driven, 2 register-resident prefetch,
+                            3 staged asynchronous copies                                        */
+  int32_t reserved[8];
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

@@ -71,6 +71,13 @@ def transpose(A: np.ndarray, B: np.ndarray, perm, size, alpha=1.0, beta=0.0, lda
     assert A.dtype == NUMPY_TYPES[ta] and B.dtype == NUMPY_TYPES[tb], (A.dtype, B.dtype, dtype)
     assert A.flags.c_contiguous and B.flags.c_contiguous
     rank = len(size)
+    from .ttc_ref import strides
+    if all(int(x) > 0 for x in size):
+        sA, sB = strides(size, perm, lda, ldb)
+        need_a = sum((int(n) - 1) * s for n, s in zip(size, sA)) + 1
+        need_b = sum((int(n) - 1) * s for n, s in zip(size, sB)) + 1
+        if A.size < need_a or B.size < need_b:
+            raise ValueError(f"buffers too small: A {A.size} < {need_a} or B {B.size} < {need_b}")
     al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
     be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
     beta_nz = 1 if complex(beta) != 0 else 0

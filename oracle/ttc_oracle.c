@@ -129,6 +129,19 @@ static inline void update(int ta, int tb, int beta_nz, const void* a, void* b, c
 
 static int esize(int t) { return t == OS ? 4 : (t == OZ ? 16 : 8); }
 
+/* Argument checks of ttc.py:733-768: perm is a permutation, lda[i] >= size[i], ldb[j] >= size[perm[j]]. */
+static int check_args(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb) {
+  int seen[16] = {0}, i;
+  for (i = 0; i < rank; ++i) {
+    if (perm[i] < 0 || perm[i] >= rank || seen[perm[i]]) return -1;
+    seen[perm[i]] = 1;
+    if (size[i] < 0) return -1;
+    if (lda && lda[i] < size[i]) return -1;
+    if (ldb && ldb[i] < size[perm[i]]) return -1;
+  }
+  return 0;
+}
+
 /*
  * Returns 0 on success, -1 on invalid arguments. size/lda/ldb/perm follow TTC's conventions;
  * lda/ldb may be NULL (dense). alpha/beta point to {re, im} pairs (im ignored for real types).
@@ -139,7 +152,7 @@ int ttco_transpose(int rank, const int* perm, const int64_t* size, const int64_t
                    const void* A, void* B) {
   int64_t sA[16], sBpos[16], sB[16], idx[16];
   int i, j;
-  if (rank < 1 || rank > 16) return -1;
+  if (rank < 1 || rank > 16 || check_args(rank, perm, size, lda, ldb)) return -1;
   sA[0] = 1;
   sBpos[0] = 1;
   for (i = 1; i < rank; ++i) {
@@ -180,7 +193,7 @@ int ttco_transpose_par(int rank, const int* perm, const int64_t* size, const int
                        const void* A, void* B, int nthreads) {
   int64_t sA[16], sBpos[16], sB[16];
   int i, j;
-  if (rank < 1 || rank > 16) return -1;
+  if (rank < 1 || rank > 16 || check_args(rank, perm, size, lda, ldb)) return -1;
   sA[0] = 1;
   sBpos[0] = 1;
   for (i = 1; i < rank; ++i) {

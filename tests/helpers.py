@@ -49,7 +49,16 @@ def bits(x: np.ndarray) -> np.ndarray:
 
 
 def assert_bitexact(got: np.ndarray, want: np.ndarray, what=""):
-    gb, wb = bits(got), bits(want)
+    """Bit-for-bit equality, except that NaN payloads are not compared (the GPU returns its
+    canonical NaN where the host propagates an operand's payload; IEEE 754 leaves this open)."""
+    gb, wb = bits(got).copy(), bits(want).copy()
+    real = np.float32 if gb.dtype == np.uint32 else np.float64
+    gn, wn = np.isnan(gb.view(real)), np.isnan(wb.view(real))
+    if not np.array_equal(gn, wn):
+        i = int(np.nonzero(gn != wn)[0][0])
+        raise AssertionError(f"{what}: NaN positions differ, first at word {i}")
+    gb[gn] = 0
+    wb[wn] = 0
     if not np.array_equal(gb, wb):
         bad = np.nonzero(gb != wb)[0]
         i = int(bad[0])

@@ -69,7 +69,8 @@ def fdiv(n, fd):
 def parse_tile(b):
     L = layout()
     names = ["P", "LA", "LB", "nsegA", "nsegB", "pshift", "pad", "phys_size", "ngrid", "nblocked", "ntiles",
-             "off_segA", "off_segB", "off_perm", "smem_bytes"]
+             "off_segA", "off_segB", "off_perm", "smem_bytes", "fast", "async_ok", "padA", "stage_elems",
+             "nstages", "off_gtab"]
     t = {k: _i32(b, 4 * i) for i, k in enumerate(names)}
     t["divLA"] = _fd(b, L["off_divLA"])
     t["divLB"] = _fd(b, L["off_divLA"] + L["fastdiv_size"])
@@ -87,7 +88,26 @@ def parse_tile(b):
     t["segA"] = np.frombuffer(b, dtype=np.int64, count=t["nsegA"], offset=t["off_segA"])
     t["segB"] = np.frombuffer(b, dtype=np.int64, count=t["nsegB"], offset=t["off_segB"])
     t["ptab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_perm"]).astype(np.int64)
+    t["gtab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_gtab"]).astype(np.int64)
     return t
+
+
+def check_staged_layout(t, vecA):
+    """The staged kernel's gather table must read, for B position q, the element that the load
+    phase copied from A position p(q) (staged at p + (p // LA) * padA), with vector-aligned copies."""
+    P = t["P"]
+    q = np.arange(P, dtype=np.int64)
+    slot_q = q + ((q >> t["pshift"]) if t["pad"] else 0)
+    inv = np.full(t["phys_size"], -1, np.int64)
+    inv[t["ptab"]] = np.arange(P, dtype=np.int64)
+    p_of_q = inv[slot_q]
+    assert (p_of_q >= 0).all()
+    stg = p_of_q + (p_of_q // t["LA"]) * t["padA"]
+    assert np.array_equal(stg, t["gtab"]), "gtab disagrees with the staged layout"
+    assert len(np.unique(t["gtab"])) == P and t["gtab"].max() < t["stage_elems"]
+    assert t["stage_elems"] >= t["phys_size"]
+    p = np.arange(0, P, vecA, dtype=np.int64)
+    assert ((p + (p // t["LA"]) * t["padA"]) % vecA == 0).all(), "staged vectors misaligned"
 
 
 def parse_row(b):
@@ -171,7 +191,13 @@ def simulate_row(r):
 def simulate(perm, size, dtype="s", beta=False, lda=None, ldb=None, tuning=None):
     kind, b = host_desc(perm, size, dtype, beta, lda, ldb, tuning)
     if kind == 1:
-        return kind, simulate_tile(parse_tile(b))
+        t = parse_tile(b)
+        if t["async_ok"]:
+            import json
+            from ttc_b200 import plan_host_json
+            j = plan_host_json(perm, size, dtype, beta, lda, ldb, tuning)
+            check_staged_layout(t, j["vecA"])
+        return kind, simulate_tile(t)
     if kind == 2:
         return kind, simulate_row(parse_row(b))
     return kind, (np.zeros(0, np.int64), np.zeros(0, np.int64))

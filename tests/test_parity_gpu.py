@@ -76,7 +76,7 @@ def test_padded_lda_ldb_and_complex_beta(dtype):
     cplx = ta in "cz"
     alpha = complex(1.25, -0.75) if cplx else 1.25
     beta = complex(-0.5, 0.3) if cplx else -0.5
-    check_case([2, 0, 3, 1], [13, 9, 6, 11], dtype, alpha, beta, lda=[16, 10, 6, 12], ldb=[6, 15, 9, 11])
+    check_case([2, 0, 3, 1], [13, 9, 6, 11], dtype, alpha, beta, lda=[16, 10, 6, 12], ldb=[6, 15, 12, 9])
     check_case([1, 2, 0], [33, 17, 9], dtype, alpha, 0.0, ldb=[17, 12, 33])
 
 

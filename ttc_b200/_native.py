@@ -34,7 +34,7 @@ class TTCError(RuntimeError):
 class Tuning(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("tile_elems", ctypes.c_int32), ("run_bytes", ctypes.c_int32),
                 ("vec", ctypes.c_int32), ("blocks", ctypes.c_int32), ("loop_order", ctypes.c_int32),
-                ("streaming", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+                ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":

@@ -78,16 +78,9 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
   e = cudaMemcpy(p->dev_desc, p->host_desc.data(), p->host_desc.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy of the plan descriptor");
 
-  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, p->kernel, p->vecA, p->vecB, variant_of(p));
-  if (!k.func) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (p->smem_bytes > 48 * 1024) allow_large_smem(k.func);
   int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, p->smem_bytes);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
   int64_t work = 1;
   if (p->kernel == TTCB_KERNEL_TILE) {
     work = reinterpret_cast<const TileDesc*>(p->host_desc.data())->ntiles;
@@ -95,16 +88,39 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     work = (rd->nunits + (ttcb::kThreads / 32) - 1) / (ttcb::kThreads / 32);  // one warp per unit
   }
-  int64_t resident = (int64_t)per_sm * sms;
-  int64_t blocks;
-  if (p->tuning.blocks > 0) {
-    blocks = std::min<int64_t>(p->tuning.blocks, work);
-  } else {
-    int64_t per = (work + resident - 1) / resident;  // work items per CTA, balanced
-    blocks = (work + per - 1) / per;
+  auto grid_for = [&](int kernel_id, int smem, int* out) -> ttcb_status {
+    ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel_id, p->vecA, p->vecB, variant_of(p));
+    if (!k.func) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
+    if (smem > 48 * 1024) allow_large_smem(k.func);
+    int per_sm = 0;
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, smem);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
+    int64_t resident = (int64_t)per_sm * sms;
+    int64_t blocks;
+    if (p->tuning.blocks > 0) {
+      blocks = std::min<int64_t>(p->tuning.blocks, work);
+    } else {
+      int64_t per = (work + resident - 1) / resident;  // work items per CTA, balanced
+      blocks = (work + per - 1) / per;
+    }
+    *out = (int)std::max<int64_t>(blocks, 1);
+    return TTCB_OK;
+  };
+  ttcb_status s = grid_for(p->kernel, p->smem_bytes, &p->blocks);
+  if (s != TTCB_OK) return s;
+  if (p->kernel == TTCB_KERNEL_TILE) {
+    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    if (td->fast) {
+      s = grid_for(TTCB_KERNEL_TILE_FAST, p->smem_fast, &p->blocks_fast);
+      if (s != TTCB_OK) return s;
+    }
+    if (td->async_ok) {
+      s = grid_for(td->nstages == 3 ? TTCB_KERNEL_TILE_ASYNC3 : TTCB_KERNEL_TILE_ASYNC2, p->smem_async,
+                   &p->blocks_async);
+      if (s != TTCB_OK) return s;
+    }
   }
-  if (blocks < 1) blocks = 1;
-  p->blocks = (int)blocks;
   return TTCB_OK;
 }
 
@@ -181,17 +197,28 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
     return fail(TTCB_ERR_INVALID_ARG, "plan was created on device " + std::to_string(p->device) +
                                           " but the current device is " + std::to_string(dev));
   int va = p->vecA, vb = p->vecB;
-  if (p->kernel == TTCB_KERNEL_ROW) {
-    const int bytes = va * std::max(EA, EB);
-    if ((uintptr_t)A % (va * EA) || (uintptr_t)B % (vb * EB) || bytes > 16) va = vb = 1;
-  } else {
-    if ((uintptr_t)A % (va * EA)) va = 1;
-    if ((uintptr_t)B % (vb * EB)) vb = 1;
+  while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
+  while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
+  if (p->kernel == TTCB_KERNEL_ROW) va = vb = std::min(va, vb);
+  int kernel = p->kernel, blocks = p->blocks, smem = p->smem_bytes;
+  if (kernel == TTCB_KERNEL_TILE) {
+    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    const int want = p->tuning.tile_variant;
+    const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
+    if ((want == 0 || want == 3) && td->async_ok) {
+      kernel = td->nstages == 3 ? TTCB_KERNEL_TILE_ASYNC3 : TTCB_KERNEL_TILE_ASYNC2;
+      blocks = p->blocks_async;
+      smem = p->smem_async;
+    } else if ((want == 0 || want == 2) && fast_ok) {
+      kernel = TTCB_KERNEL_TILE_FAST;
+      blocks = p->blocks_fast;
+      smem = p->smem_fast;
+    }
   }
-  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, p->kernel, va, vb, variant_of(p));
+  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel, va, vb, variant_of(p));
   if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (p->smem_bytes > 48 * 1024) allow_large_smem(k.func);
-  e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), p->blocks);
+  if (smem > 48 * 1024) allow_large_smem(k.func);
+  e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), blocks);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return TTCB_OK;
 }

@@ -31,11 +31,12 @@ __device__ __forceinline__ void batch_tile(const BatchProblem& bp, uint32_t t, T
   TB* B = static_cast<TB*>(bp.B);
   constexpr int MA = 16 / sizeof(TA);
   constexpr int MB = 16 / sizeof(TB);
-  if (bp.va > 1 && bp.vb > 1)
+  // the widest access each side allows (16 bytes) or scalar; narrower plans run scalar here
+  if (bp.va == MA && bp.vb == MB)
     tile_body<TA, TB, MA, MB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-  else if (bp.va > 1)
+  else if (bp.va == MA)
     tile_body<TA, TB, MA, 1, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-  else if (bp.vb > 1)
+  else if (bp.vb == MB)
     tile_body<TA, TB, 1, MB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
   else
     tile_body<TA, TB, 1, 1, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
@@ -52,7 +53,7 @@ __device__ __forceinline__ void batch_row(const BatchProblem& bp, uint32_t item,
   constexpr int MR = MA < MB ? MA : MB;
   const TA* A = static_cast<const TA*>(bp.A);
   TB* B = static_cast<TB*>(bp.B);
-  if (bp.va > 1)
+  if (bp.va == MR && bp.vb == MR)
     row_unit<TA, TB, MR, BETA, STREAM>(d, u, A, B, alpha, beta, lane);
   else
     row_unit<TA, TB, 1, BETA, STREAM>(d, u, A, B, alpha, beta, lane);

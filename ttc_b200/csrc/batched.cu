@@ -149,13 +149,13 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
       q.kind = p->kernel;
       q.va = p->vecA;
       q.vb = p->vecB;
+      while (q.va > 1 && (uintptr_t)A[i] % (q.va * EA)) q.va /= 2;
+      while (q.vb > 1 && (uintptr_t)B[i] % (q.vb * EB)) q.vb /= 2;
       if (p->kernel == TTCB_KERNEL_ROW) {
-        if ((uintptr_t)A[i] % (q.va * EA) || (uintptr_t)B[i] % (q.vb * EB)) q.va = q.vb = 1;
+        q.va = q.vb = std::min(q.va, q.vb);
         const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
         items = (rd->nunits + 7) / 8;
       } else {
-        if ((uintptr_t)A[i] % (q.va * EA)) q.va = 1;
-        if ((uintptr_t)B[i] % (q.vb * EB)) q.vb = 1;
         const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
         items = td->ntiles;
         max_slots_bytes = std::max<int>(max_slots_bytes, (int)ttcb::tile_slots_bytes(td->phys_size, EA));

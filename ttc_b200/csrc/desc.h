@@ -48,8 +48,16 @@ struct TileDesc {
   int32_t off_segA;   // byte offsets of the tables, relative to the start of the descriptor
   int32_t off_segB;
   int32_t off_perm;
-  int32_t smem_bytes; // dynamic shared memory the kernel needs
-  int32_t pad_[1];
+  int32_t smem_bytes; // dynamic shared memory the generic kernel needs (slots + tables)
+  int32_t fast;       // 1: every tile-relative offset fits in 32 bits and the fast kernel applies
+  // staged (asynchronous-copy) kernel: A tiles land in shared memory in A order, element p at
+  // p + (p / LA) * padA; the store phase gathers B order through gtab[q]
+  int32_t async_ok;   // 1: the staged kernel applies (32-bit offsets, <= 16 elements per thread)
+  int32_t padA;       // padding after each A run in the staged layout (multiple of the A vector)
+  int32_t stage_elems;// elements of one stage buffer (max of the staged layout and phys_size)
+  int32_t nstages;    // pipeline depth (2 or 3)
+  int32_t off_gtab;   // byte offset of gtab (uint16_t[P]) from the start of the descriptor
+  int32_t pad2_[3];
   FastDiv divLA, divLB;
   GridDimDesc g[TTCB_MAXR];
   BlockedDesc bd[2];
@@ -69,3 +77,5 @@ struct RowDesc {
 };
 
 enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };
+// launch-time variant of a tile plan (never stored in a plan's kernel field)
+enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC2 = 4, TTCB_KERNEL_TILE_ASYNC3 = 5 };

@@ -57,8 +57,99 @@ struct TileTables {
   const uint16_t* ptab;
 };
 
-// One tile: load phase (A runs -> alpha*A -> shared slots in B order), barrier, store phase
-// (shared slots -> B runs, with beta*B when BETA), barrier. All threads of the CTA take part.
+// out[j] = v[(j + r) mod V] for a run-time r in [0, V): two select stages, registers only.
+template <typename T, int V> __device__ __forceinline__ Vec<T, V> rot_left(const Vec<T, V>& v, int r) {
+  Vec<T, V> a = v;
+  if constexpr (V >= 2) {
+    Vec<T, V> b;
+#pragma unroll
+    for (int j = 0; j < V; ++j) b.v[j] = (r & 1) ? a.v[(j + 1) % V] : a.v[j];
+    a = b;
+  }
+  if constexpr (V >= 4) {
+    Vec<T, V> b;
+#pragma unroll
+    for (int j = 0; j < V; ++j) b.v[j] = (r & 2) ? a.v[(j + 2) % V] : a.v[j];
+    a = b;
+  }
+  return a;
+}
+
+// Ragged tile (a blocked dimension's last block): element-wise, validity from the blocked
+// dimensions' tile coordinates. Ends with a barrier.
+template <typename TA, typename TB, bool BETA, bool STREAM>
+__device__ __forceinline__ void tile_ragged(const TileDesc& d, const TileTables& tt, const int* lim, const TA* __restrict__ At,
+                                         TB* __restrict__ Bt, TA alpha, TB beta, TA* tile) {
+  const int tid = threadIdx.x;
+  const int P = d.P, LA = d.LA, LB = d.LB;
+  const int pshift = d.pshift, pad = d.pad;
+  const int nb = d.nblocked;
+  for (int p0 = tid; p0 < P; p0 += kThreads * kUnroll) {
+    TA v[kUnroll];
+    int slot[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int p = p0 + u * kThreads;
+      slot[u] = -1;
+      if (p < P) {
+        bool ok = true;
+        for (int b = 0; b < nb; ++b) {
+          const uint32_t c = fdiv((uint32_t)p, d.bd[b].tsA);
+          const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
+          ok = ok && ((int)cc < lim[b]);
+        }
+        if (ok) {
+          const int s = (int)fdiv((uint32_t)p, d.divLA);
+          v[u] = ld_scalar<TA>(At + (tt.segA[s] + (p - s * LA)));
+          slot[u] = tt.ptab[p];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (slot[u] >= 0) tile[slot[u]] = scale_a(alpha, v[u]);
+  }
+  __syncthreads();
+  for (int q0 = tid; q0 < P; q0 += kThreads * kUnroll) {
+    TB* dst[kUnroll];
+    TB bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int q = q0 + u * kThreads;
+      dst[u] = nullptr;
+      if (q < P) {
+        bool ok = true;
+        for (int b = 0; b < nb; ++b) {
+          const uint32_t c = fdiv((uint32_t)q, d.bd[b].tsB);
+          const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
+          ok = ok && ((int)cc < lim[b]);
+        }
+        if (ok) {
+          const int s = (int)fdiv((uint32_t)q, d.divLB);
+          dst[u] = Bt + (tt.segB[s] + (q - s * LB));
+          if (BETA) bv[u] = ld_scalar<TB>(dst[u]);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (dst[u]) {
+        const int q = q0 + u * kThreads;
+        const TA tq = tile[slot_of(q, pshift, pad)];
+        TB r;
+        if (BETA)
+          r = combine<TA, TB>(tq, bv[u], beta);
+        else
+          r = finish<TA, TB>(tq);
+        st_scalar<TB>(dst[u], r, STREAM);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// One tile with the generic table-driven loops: load phase (A runs -> alpha*A -> shared slots in B
+// order), barrier, store phase (shared slots -> B runs, with beta*B when BETA), barrier.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM>
 __device__ __forceinline__ void tile_body(const TileDesc& d, const TileTables& tt, uint32_t t, const TA* __restrict__ A,
                                           TB* __restrict__ B, TA alpha, TB beta, TA* tile) {
@@ -71,118 +162,85 @@ __device__ __forceinline__ void tile_body(const TileDesc& d, const TileTables& t
   const bool full = decode_tile(d, t, bA, bB, lim);
   const TA* At = A + bA;
   TB* Bt = B + bB;
-  if (full) {
-    const int nvA = P / VA;
-    for (int i0 = tid; i0 < nvA; i0 += kThreads * kUnroll) {
-      Vec<TA, VA> v[kUnroll];
+  if (!full) {
+    tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, At, Bt, alpha, beta, tile);
+    return;
+  }
+  const int nvA = P / VA;
+  for (int i0 = tid; i0 < nvA; i0 += kThreads * kUnroll) {
+    Vec<TA, VA> v[kUnroll];
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const int i = i0 + u * kThreads;
-        if (i < nvA) {
-          const int p = i * VA;
-          const int s = (int)fdiv((uint32_t)p, d.divLA);
-          v[u] = ld_stream<TA, VA>(At + (tt.segA[s] + (p - s * LA)));
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const int i = i0 + u * kThreads;
-        if (i < nvA) {
-          const int p = i * VA;
-#pragma unroll
-          for (int j = 0; j < VA; ++j) {
-            const int jj = (j + rot) & (VA - 1);
-            tile[tt.ptab[p + jj]] = scale_a(alpha, vsel<TA, VA>(v[u], jj));
-          }
-        }
-      }
-    }
-    __syncthreads();
-    const int nvB = P / VB;
-    for (int i0 = tid; i0 < nvB; i0 += kThreads * kUnroll) {
-      int64_t o[kUnroll];
-      Vec<TB, VB> bv[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const int i = i0 + u * kThreads;
-        if (i < nvB) {
-          const int q = i * VB;
-          const int s = (int)fdiv((uint32_t)q, d.divLB);
-          o[u] = tt.segB[s] + (q - s * LB);
-          if (BETA) bv[u] = ld_stream<TB, VB>(Bt + o[u]);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const int i = i0 + u * kThreads;
-        if (i < nvB) {
-          const int q = i * VB;
-          Vec<TA, VB> tv;
-#pragma unroll
-          for (int j = 0; j < VB; ++j) {
-            const int jj = (j + rot) & (VB - 1);
-            tv.v[j] = tile[slot_of(q + jj, pshift, pad)];
-          }
-          Vec<TB, VB> out;
-#pragma unroll
-          for (int k = 0; k < VB; ++k) {
-            const TA tk = vsel<TA, VB>(tv, (k - rot) & (VB - 1));
-            if (BETA)
-              out.v[k] = combine<TA, TB>(tk, bv[u].v[k], beta);
-            else
-              out.v[k] = finish<TA, TB>(tk);
-          }
-          st_vec<TB, VB>(Bt + o[u], out, STREAM);
-        }
-      }
-    }
-  } else {
-    // ragged tile: element-wise, validity from the blocked dimensions' tile coordinates
-    const int nb = d.nblocked;
-    for (int p = tid; p < P; p += kThreads) {
-      bool ok = true;
-      for (int b = 0; b < nb; ++b) {
-        const uint32_t c = fdiv((uint32_t)p, d.bd[b].tsA);
-        const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-        ok = ok && ((int)cc < lim[b]);
-      }
-      if (ok) {
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = i0 + u * kThreads;
+      if (i < nvA) {
+        const int p = i * VA;
         const int s = (int)fdiv((uint32_t)p, d.divLA);
-        tile[tt.ptab[p]] = scale_a(alpha, ld_scalar<TA>(At + (tt.segA[s] + (p - s * LA))));
+        v[u] = ld_stream<TA, VA>(At + (tt.segA[s] + (p - s * LA)));
       }
     }
-    __syncthreads();
-    for (int q = tid; q < P; q += kThreads) {
-      bool ok = true;
-      for (int b = 0; b < nb; ++b) {
-        const uint32_t c = fdiv((uint32_t)q, d.bd[b].tsB);
-        const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-        ok = ok && ((int)cc < lim[b]);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = i0 + u * kThreads;
+      if (i < nvA) {
+        const int p = i * VA;
+#pragma unroll
+        for (int j = 0; j < VA; ++j) {
+          const int jj = (j + rot) & (VA - 1);
+          tile[tt.ptab[p + jj]] = scale_a(alpha, vsel<TA, VA>(v[u], jj));
+        }
       }
-      if (ok) {
+    }
+  }
+  __syncthreads();
+  const int nvB = P / VB;
+  for (int i0 = tid; i0 < nvB; i0 += kThreads * kUnroll) {
+    int64_t o[kUnroll];
+    Vec<TB, VB> bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = i0 + u * kThreads;
+      if (i < nvB) {
+        const int q = i * VB;
         const int s = (int)fdiv((uint32_t)q, d.divLB);
-        TB* dst = Bt + (tt.segB[s] + (q - s * LB));
-        const TA tq = tile[slot_of(q, pshift, pad)];
-        TB r;
-        if (BETA)
-          r = combine<TA, TB>(tq, ld_scalar<TB>(dst), beta);
-        else
-          r = finish<TA, TB>(tq);
-        st_scalar<TB>(dst, r, STREAM);
+        o[u] = tt.segB[s] + (q - s * LB);
+        if (BETA) bv[u] = ld_stream<TB, VB>(Bt + o[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int i = i0 + u * kThreads;
+      if (i < nvB) {
+        const int q = i * VB;
+        Vec<TA, VB> tv;
+#pragma unroll
+        for (int j = 0; j < VB; ++j) {
+          const int jj = (j + rot) & (VB - 1);
+          tv.v[j] = tile[slot_of(q + jj, pshift, pad)];
+        }
+        Vec<TB, VB> out;
+#pragma unroll
+        for (int k = 0; k < VB; ++k) {
+          const TA tk = vsel<TA, VB>(tv, (k - rot) & (VB - 1));
+          if (BETA)
+            out.v[k] = combine<TA, TB>(tk, bv[u].v[k], beta);
+          else
+            out.v[k] = finish<TA, TB>(tk);
+        }
+        st_vec<TB, VB>(Bt + o[u], out, STREAM);
       }
     }
   }
   __syncthreads();
 }
 
-// Shared-memory layout of the plain tile kernel: [tile slots][segA][segB][perm_tab].
+// Shared-memory layout of the generic tile kernel: [tile slots][segA][segB][perm_tab].
 __host__ __device__ inline size_t tile_slots_bytes(int phys_size, int elem_bytes) {
   return ((size_t)phys_size * elem_bytes + 15) & ~size_t(15);
 }
 
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM>
 __global__ void __launch_bounds__(kThreads, 4) tile_kernel(const TileDesc* __restrict__ desc, const TA* __restrict__ A,
-                                                        TB* __restrict__ B, TA alpha, TB beta) {
+                                                           TB* __restrict__ B, TA alpha, TB beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const TileDesc& d = *desc;
   const int tid = threadIdx.x;
@@ -205,6 +263,289 @@ __global__ void __launch_bounds__(kThreads, 4) tile_kernel(const TileDesc* __res
   const uint32_t ntiles = (uint32_t)d.ntiles;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x)
     tile_body<TA, TB, VA, VB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Fast tile kernel. Each thread owns up to kMaxVec A-vectors and kMaxVec B-vectors of every tile;
+// their tile-relative offsets and shared-memory slots do not depend on the tile, so they are
+// computed once per CTA and kept in registers. The A loads of the next tile are issued before the
+// store phase of the current one, so loads stay in flight across the barrier. Needs P/VA and P/VB
+// <= kMaxVec * kThreads and 32-bit tile-relative offsets (TileDesc::fast).
+constexpr int kMaxVec = 4;
+
+template <typename TA, int VA>
+__device__ __forceinline__ void fast_load(Vec<TA, VA>* va, const TA* __restrict__ At, const int32_t* relA) {
+#pragma unroll
+  for (int u = 0; u < kMaxVec; ++u)
+    if (relA[u] >= 0) va[u] = ld_stream<TA, VA>(At + relA[u]);
+}
+
+template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM>
+__global__ void __launch_bounds__(kThreads, 3) tile_fast_kernel(const TileDesc* __restrict__ desc,
+                                                                const TA* __restrict__ A, TB* __restrict__ B,
+                                                                TA alpha, TB beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TA* tile = reinterpret_cast<TA*>(smem_raw);
+  const TileDesc& d = *desc;
+  const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
+  const TileTables tt{reinterpret_cast<const int64_t*>(base + d.off_segA),
+                      reinterpret_cast<const int64_t*>(base + d.off_segB),
+                      reinterpret_cast<const uint16_t*>(base + d.off_perm)};
+  const int tid = threadIdx.x;
+  const int rotA = (tid >> 3) & (VA - 1);
+  const int rotB = (tid >> 3) & (VB - 1);
+  const int P = d.P, LA = d.LA, LB = d.LB;
+  const int nvA = P / VA, nvB = P / VB;
+
+  // tile-invariant per-thread offsets and slots (A-side slots in the thread's write order, two
+  // 16-bit slots per register)
+  constexpr int NSA = (VA + 1) / 2;
+  int32_t relA[kMaxVec], relB[kMaxVec];
+  uint32_t slA[kMaxVec][NSA];
+#pragma unroll
+  for (int u = 0; u < kMaxVec; ++u) {
+    const int i = tid + u * kThreads;
+    relA[u] = -1;
+    if (i < nvA) {
+      const int p = i * VA;
+      const int s = p / LA;
+      relA[u] = (int32_t)(tt.segA[s] + (p - s * LA));
+#pragma unroll
+      for (int j = 0; j < NSA; ++j) {
+        const uint32_t lo = tt.ptab[p + ((2 * j + rotA) & (VA - 1))];
+        const uint32_t hi = (2 * j + 1 < VA) ? tt.ptab[p + ((2 * j + 1 + rotA) & (VA - 1))] : 0u;
+        slA[u][j] = lo | (hi << 16);
+      }
+    }
+    relB[u] = -1;
+    if (i < nvB) {
+      const int q = i * VB;
+      const int s = q / LB;
+      relB[u] = (int32_t)(tt.segB[s] + (q - s * LB));
+    }
+  }
+  const int pshift = d.pshift, pad = d.pad;
+
+  const uint32_t ntiles = (uint32_t)d.ntiles;
+  uint32_t t = blockIdx.x;
+  int64_t bA = 0, bB = 0;
+  int lim[2];
+  Vec<TA, VA> va[kMaxVec];
+  bool full = false;
+  if (t < ntiles) {
+    full = decode_tile(d, t, bA, bB, lim);
+    if (full) fast_load<TA, VA>(va, A + bA, relA);
+  }
+  while (t < ntiles) {
+    const uint32_t tn = t + gridDim.x;
+    int64_t nA = 0, nB = 0;
+    int nlim[2];
+    bool nfull = false;
+    if (full) {
+#pragma unroll
+      for (int u = 0; u < kMaxVec; ++u) {
+        if (relA[u] >= 0) {
+          const Vec<TA, VA> w = rot_left<TA, VA>(va[u], rotA);
+#pragma unroll
+          for (int j = 0; j < VA; ++j) {
+            const uint32_t sl = (j & 1) ? (slA[u][j >> 1] >> 16) : (slA[u][j >> 1] & 0xffffu);
+            tile[sl] = scale_a(alpha, w.v[j]);
+          }
+        }
+      }
+      __syncthreads();
+      // next tile's A loads go out before this tile's stores
+      if (tn < ntiles) {
+        nfull = decode_tile(d, tn, nA, nB, nlim);
+        if (nfull) fast_load<TA, VA>(va, A + nA, relA);
+      }
+      TB* Bt = B + bB;
+      Vec<TB, VB> bv[kMaxVec];
+      if (BETA) {
+#pragma unroll
+        for (int u = 0; u < kMaxVec; ++u)
+          if (relB[u] >= 0) bv[u] = ld_stream<TB, VB>(Bt + relB[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kMaxVec; ++u) {
+        if (relB[u] >= 0) {
+          const int slb = slot_of((tid + u * kThreads) * VB, pshift, pad);
+          Vec<TA, VB> tv;
+#pragma unroll
+          for (int j = 0; j < VB; ++j) tv.v[j] = tile[slb + ((j + rotB) & (VB - 1))];
+          tv = rot_left<TA, VB>(tv, (VB - rotB) & (VB - 1));
+          Vec<TB, VB> out;
+#pragma unroll
+          for (int k = 0; k < VB; ++k) {
+            if (BETA)
+              out.v[k] = combine<TA, TB>(tv.v[k], bv[u].v[k], beta);
+            else
+              out.v[k] = finish<TA, TB>(tv.v[k]);
+          }
+          st_vec<TB, VB>(Bt + relB[u], out, STREAM);
+        }
+      }
+      __syncthreads();
+    } else {
+      tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, A + bA, B + bB, alpha, beta, tile);
+      if (tn < ntiles) {
+        nfull = decode_tile(d, tn, nA, nB, nlim);
+        if (nfull) fast_load<TA, VA>(va, A + nA, relA);
+      }
+    }
+    t = tn;
+    full = nfull;
+    bA = nA;
+    bB = nB;
+    lim[0] = nlim[0];
+    lim[1] = nlim[1];
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Staged tile kernel. A tiles are fetched with asynchronous global->shared copies (cp.async, no
+// register cost) into an S-stage ring, so S-1 tiles of loads stay in flight per CTA while the
+// current tile is written out. Shared memory holds A in A order (element p at p + (p/LA)*padA,
+// padA chosen by the planner against bank conflicts); the store phase gathers B order through
+// gtab[q] and applies alpha (and beta*B) on the way out.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <int BYTES> __device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+  else if constexpr (BYTES == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Shared-memory layout of the staged kernel: [S stages][segA][segB][gtab].
+__host__ __device__ inline size_t stage_bytes(int stage_elems, int elem_bytes) {
+  return ((size_t)stage_elems * elem_bytes + 15) & ~size_t(15);
+}
+
+template <typename T, int V> __device__ __forceinline__ void ld_u16s(const uint16_t* p, uint16_t* out) {
+  if constexpr (V == 4) {
+    const uint2 w = *reinterpret_cast<const uint2*>(p);
+    out[0] = (uint16_t)(w.x & 0xffffu);
+    out[1] = (uint16_t)(w.x >> 16);
+    out[2] = (uint16_t)(w.y & 0xffffu);
+    out[3] = (uint16_t)(w.y >> 16);
+  } else if constexpr (V == 2) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(p);
+    out[0] = (uint16_t)(w & 0xffffu);
+    out[1] = (uint16_t)(w >> 16);
+  } else {
+    out[0] = p[0];
+  }
+}
+
+template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, int S>
+__global__ void __launch_bounds__(kThreads) tile_async_kernel(const TileDesc* __restrict__ desc,
+                                                              const TA* __restrict__ A, TB* __restrict__ B,
+                                                              TA alpha, TB beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TileDesc& d = *desc;
+  const int tid = threadIdx.x;
+  const int P = d.P, LA = d.LA, LB = d.LB, padA = d.padA;
+  const size_t sbytes = stage_bytes(d.stage_elems, sizeof(TA));
+  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + S * sbytes);
+  int64_t* segB = segA + d.nsegA;
+  uint16_t* gtab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+  const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
+  {
+    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
+    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
+    const uint32_t* gG = reinterpret_cast<const uint32_t*>(base + d.off_gtab);
+    uint32_t* sG = reinterpret_cast<uint32_t*>(gtab);
+    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
+    for (int i = tid; i < (P + 1) / 2; i += kThreads) sG[i] = gG[i];
+  }
+  const TileTables tg{reinterpret_cast<const int64_t*>(base + d.off_segA),
+                      reinterpret_cast<const int64_t*>(base + d.off_segB),
+                      reinterpret_cast<const uint16_t*>(base + d.off_perm)};
+  __syncthreads();
+
+  const uint32_t ntiles = (uint32_t)d.ntiles;
+  const uint32_t G = gridDim.x;
+  const int nvA = P / VA, nvB = P / VB;
+  const uint32_t stage0 = smem_u32(smem_raw);
+
+  auto issue = [&](uint32_t t, int stage) {
+    if (t >= ntiles) return;
+    int64_t bA, bB;
+    int lim[2];
+    if (!decode_tile(d, t, bA, bB, lim)) return;  // ragged tiles are read by the ragged path
+    const TA* At = A + bA;
+    const uint32_t sb = stage0 + (uint32_t)(stage * sbytes);
+    for (int i = tid; i < nvA; i += kThreads) {
+      const int p = i * VA;
+      const int s = (int)fdiv((uint32_t)p, d.divLA);
+      cp_async<VA * sizeof(TA)>(sb + (uint32_t)((p + s * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+    }
+  };
+
+#pragma unroll
+  for (int k = 0; k < S - 1; ++k) {
+    issue(blockIdx.x + k * G, k);
+    cp_async_commit();
+  }
+  for (uint32_t k = 0;; ++k) {
+    const uint32_t t = blockIdx.x + k * G;
+    if (t >= ntiles) break;
+    issue(t + (S - 1) * G, (int)((k + S - 1) % S));
+    cp_async_commit();
+    int64_t bA, bB;
+    int lim[2];
+    const bool full = decode_tile(d, t, bA, bB, lim);
+    TB* Bt = B + bB;
+    TA* st = reinterpret_cast<TA*>(smem_raw + (k % S) * sbytes);
+    cp_async_wait<S - 1>();
+    __syncthreads();
+    if (full) {
+      for (int i0 = tid; i0 < nvB; i0 += kThreads * kUnroll) {
+        int64_t o[kUnroll];
+        Vec<TB, VB> bv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const int i = i0 + u * kThreads;
+          if (i < nvB) {
+            const int q = i * VB;
+            const int s = (int)fdiv((uint32_t)q, d.divLB);
+            o[u] = segB[s] + (q - s * LB);
+            if (BETA) bv[u] = ld_stream<TB, VB>(Bt + o[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const int i = i0 + u * kThreads;
+          if (i < nvB) {
+            uint16_t pos[VB];
+            ld_u16s<TA, VB>(gtab + i * VB, pos);
+            Vec<TB, VB> out;
+#pragma unroll
+            for (int j = 0; j < VB; ++j) {
+              const TA tj = scale_a(alpha, st[pos[j]]);
+              if (BETA)
+                out.v[j] = combine<TA, TB>(tj, bv[u].v[j], beta);
+              else
+                out.v[j] = finish<TA, TB>(tj);
+            }
+            st_vec<TB, VB>(Bt + o[u], out, STREAM);
+          }
+        }
+      }
+    } else {
+      tile_ragged<TA, TB, BETA, STREAM>(d, tg, lim, A + bA, Bt, alpha, beta, st);
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
 }
 
 // One row-copy work unit (row, chunk) processed by one warp.

@@ -53,7 +53,52 @@ using TB = float2;
 #define PAIR_BATCH_FN pick_batch_zc
 #endif
 
-template <int VA, int VB, bool BETA, bool STREAM>
+template <int VA, int VB, bool BETA, bool STREAM, int S>
+static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
+                                cudaStream_t stream, int blocks) {
+  TA al;
+  std::memcpy(&al, alpha, sizeof(TA));
+  TB be;
+  std::memset(&be, 0, sizeof(TB));
+  if (BETA) std::memcpy(&be, beta, sizeof(TB));
+  tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, S><<<blocks, kThreads, p->smem_async, stream>>>(
+      reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
+  return cudaGetLastError();
+}
+
+template <int VA, int VB, int S>
+static KernelRef async_ref(int variant) {
+  KernelRef r;
+  if (variant == 2) {
+    r.fn = &launch_async<VA, VB, true, false, S>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, S>);
+  } else if (variant == 1) {
+    r.fn = &launch_async<VA, VB, false, true, S>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, S>);
+  } else {
+    r.fn = &launch_async<VA, VB, false, false, S>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, S>);
+  }
+  return r;
+}
+
+template <int VA, int S>
+static KernelRef async_ref_b(int vb, int variant) {
+  constexpr int MB = 16 / sizeof(TB);
+  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), S>(variant);
+  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), S>(variant);
+  return async_ref<VA, 1, S>(variant);
+}
+
+template <int S>
+static KernelRef async_ref_ab(int va, int vb, int variant) {
+  constexpr int MA = 16 / sizeof(TA);
+  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), S>(vb, variant);
+  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), S>(vb, variant);
+  return async_ref_b<1, S>(vb, variant);
+}
+
+template <int VA, int VB, bool BETA, bool STREAM, bool FAST>
 static cudaError_t launch_tile(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
                                cudaStream_t stream, int blocks) {
   TA al;
@@ -61,8 +106,13 @@ static cudaError_t launch_tile(const ttcb_plan* p, const void* A, void* B, const
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
-  tile_kernel<TA, TB, VA, VB, BETA, STREAM><<<blocks, kThreads, p->smem_bytes, stream>>>(
-      reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
+  const TileDesc* d = reinterpret_cast<const TileDesc*>(p->dev_desc);
+  if (FAST)
+    tile_fast_kernel<TA, TB, VA, VB, BETA, STREAM><<<blocks, kThreads, p->smem_fast, stream>>>(
+        d, static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
+  else
+    tile_kernel<TA, TB, VA, VB, BETA, STREAM><<<blocks, kThreads, p->smem_bytes, stream>>>(
+        d, static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
   return cudaGetLastError();
 }
 
@@ -79,20 +129,39 @@ static cudaError_t launch_row(const ttcb_plan* p, const void* A, void* B, const 
   return cudaGetLastError();
 }
 
-template <int VA, int VB>
+template <int VA, int VB, bool FAST>
 static KernelRef tile_ref(int variant) {
   KernelRef r;
   if (variant == 2) {
-    r.fn = &launch_tile<VA, VB, true, false>;
-    r.func = reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, true, false>);
+    r.fn = &launch_tile<VA, VB, true, false, FAST>;
+    r.func = FAST ? reinterpret_cast<const void*>(&tile_fast_kernel<TA, TB, VA, VB, true, false>)
+                  : reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, true, false>);
   } else if (variant == 1) {
-    r.fn = &launch_tile<VA, VB, false, true>;
-    r.func = reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, false, true>);
+    r.fn = &launch_tile<VA, VB, false, true, FAST>;
+    r.func = FAST ? reinterpret_cast<const void*>(&tile_fast_kernel<TA, TB, VA, VB, false, true>)
+                  : reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, false, true>);
   } else {
-    r.fn = &launch_tile<VA, VB, false, false>;
-    r.func = reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, false, false>);
+    r.fn = &launch_tile<VA, VB, false, false, FAST>;
+    r.func = FAST ? reinterpret_cast<const void*>(&tile_fast_kernel<TA, TB, VA, VB, false, false>)
+                  : reinterpret_cast<const void*>(&tile_kernel<TA, TB, VA, VB, false, false>);
   }
   return r;
+}
+
+template <int VA, bool FAST>
+static KernelRef tile_ref_b(int vb, int variant) {
+  constexpr int MB = 16 / sizeof(TB);
+  if (vb >= 4 && MB >= 4) return tile_ref<VA, (MB >= 4 ? 4 : 1), FAST>(variant);
+  if (vb >= 2 && MB >= 2) return tile_ref<VA, (MB >= 2 ? 2 : 1), FAST>(variant);
+  return tile_ref<VA, 1, FAST>(variant);
+}
+
+template <bool FAST>
+static KernelRef tile_ref_ab(int va, int vb, int variant) {
+  constexpr int MA = 16 / sizeof(TA);
+  if (va >= 4 && MA >= 4) return tile_ref_b<(MA >= 4 ? 4 : 1), FAST>(vb, variant);
+  if (va >= 2 && MA >= 2) return tile_ref_b<(MA >= 2 ? 2 : 1), FAST>(vb, variant);
+  return tile_ref_b<1, FAST>(vb, variant);
 }
 
 template <int V>
@@ -116,14 +185,15 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
   constexpr int MB = 16 / sizeof(TB);
   constexpr int MR = MA < MB ? MA : MB;
   if (kernel == TTCB_KERNEL_ROW) {
-    if (va > 1 && vb > 1) return row_ref<MR>(variant);
+    const int v = va < vb ? va : vb;
+    if (v >= 4 && MR >= 4) return row_ref<(MR >= 4 ? 4 : 1)>(variant);
+    if (v >= 2 && MR >= 2) return row_ref<(MR >= 2 ? 2 : 1)>(variant);
     return row_ref<1>(variant);
   }
-  const bool a = va > 1, b = vb > 1;
-  if (a && b) return tile_ref<MA, MB>(variant);
-  if (a) return tile_ref<MA, 1>(variant);
-  if (b) return tile_ref<1, MB>(variant);
-  return tile_ref<1, 1>(variant);
+  if (kernel == TTCB_KERNEL_TILE_FAST) return tile_ref_ab<true>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC2) return async_ref_ab<2>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC3) return async_ref_ab<3>(va, vb, variant);
+  return tile_ref_ab<false>(va, vb, variant);
 }
 
 template <bool BETA, bool STREAM>

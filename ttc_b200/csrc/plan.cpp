@@ -181,9 +181,18 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   }
   c.galA = gA;
   c.galB = gB;
-  int VA = 16 / EA, VB = 16 / EB;
-  c.vecA = (VA > 1 && c.LA % VA == 0 && (gA == 0 || gA % VA == 0)) ? VA : 1;
-  c.vecB = (VB > 1 && c.LB % VB == 0 && (gB == 0 || gB % VB == 0)) ? VB : 1;
+  c.vecA = 1;
+  for (int V = 16 / EA; V > 1; V /= 2)
+    if (c.LA % V == 0 && (gA == 0 || gA % V == 0)) {
+      c.vecA = V;
+      break;
+    }
+  c.vecB = 1;
+  for (int V = 16 / EB; V > 1; V /= 2)
+    if (c.LB % V == 0 && (gB == 0 || gB % V == 0)) {
+      c.vecB = V;
+      break;
+    }
   if (tu.vec == 1) c.vecA = c.vecB = 1;
 
   int64_t alA = gA == 0 ? 128 : std::min<int64_t>(128, (gA * EA) & -(gA * EA));
@@ -191,8 +200,12 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   double effA = run_eff((double)c.LA * EA, alA);
   double effB = run_eff((double)c.LB * EB, alB);
   double per_elem = EA / effA + (beta ? 2.0 : 1.0) * EB / effB;
-  if (c.vecA == 1 && EA < 16) per_elem += 0.15 * EA;  // more instructions per byte
-  if (c.vecB == 1 && EB < 16) per_elem += 0.15 * EB * (beta ? 2.0 : 1.0);
+  // narrower accesses cost issue slots (the kernels are close to instruction-bound)
+  per_elem += 0.6 * EA * (16.0 / (c.vecA * EA) - 1.0) / 15.0 * 4.0;
+  per_elem += 0.6 * EB * (16.0 / (c.vecB * EB) - 1.0) / 15.0 * 4.0 * (beta ? 1.5 : 1.0);
+  // the fast kernel keeps at most 4 vectors per thread and phase
+  const bool fast = (c.P / c.vecA <= 1024) && (c.P / c.vecB <= 1024);
+  if (!fast) per_elem *= 1.6;
 
   // average useful elements per tile (ragged last blocks waste a tile's fixed cost)
   double fill = 1.0;
@@ -208,6 +221,16 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   }
   double tile_overhead = 3072.0;  // bytes-equivalent per tile
   double cost = per_elem + tile_overhead / (c.P * fill);
+  // last blocks of blocked dimensions run the element-wise ragged path
+  {
+    double full_frac = 1.0;
+    for (int d = 0; d < f.rank; ++d)
+      if (c.ext[d] > 0 && c.ext[d] < f.n[d] && f.n[d] % c.ext[d] != 0) {
+        int64_t nb = (f.n[d] + c.ext[d] - 1) / c.ext[d];
+        full_frac *= (double)(nb - 1) / (double)nb;
+      }
+    cost += (1.0 - full_frac) * per_elem * 1.5;
+  }
 
   // shared memory footprint and residency
   int64_t nsegA = c.P / c.LA, nsegB = c.P / c.LB;
@@ -337,6 +360,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   int64_t nsegA = P / c.LA, nsegB = P / c.LB;
   std::vector<int64_t> segA(nsegA), segB(nsegB);
   std::vector<uint16_t> ptab(P);
+  std::vector<int64_t> p_of_q(P);
   for (int64_t pp = 0; pp < P; ++pp) {
     int64_t rem = pp, offA = 0, q = 0;
     for (int d : aord) {
@@ -346,8 +370,51 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       q += cd * tsB[d];
     }
     ptab[pp] = (uint16_t)phys(q);
+    p_of_q[q] = pp;
     if (pp % c.LA == 0) segA[pp / c.LA] = offA;
   }
+  // Staged layout of the asynchronous-copy kernel: element p at p + (p / LA) * padA. The pad is the
+  // multiple of the A vector that minimises shared-memory bank conflicts of the store-phase gather,
+  // replayed on the host for the first warps (32 lanes, 4-byte banks).
+  const int EAw = EA >= 4 ? EA / 4 : 1;
+  auto staged = [&](int64_t pp, int64_t padA) { return pp + (pp / c.LA) * padA; };
+  auto gather_cost = [&](int64_t padA) {
+    int64_t cost = 0;
+    const int vb = c.vecB;
+    for (int w = 0; w < 4; ++w) {
+      for (int j = 0; j < vb; ++j) {
+        int cnt[32] = {0};
+        int mx = 0;
+        for (int lane = 0; lane < 32; ++lane) {
+          int64_t i = (int64_t)w * 32 + lane;
+          if (i * vb >= P) continue;
+          int64_t word = staged(p_of_q[i * vb + j], padA) * EAw;
+          for (int x = 0; x < EAw; ++x) {
+            int b = (int)((word + x) & 31);
+            mx = std::max(mx, ++cnt[b]);
+          }
+        }
+        cost += mx;
+      }
+    }
+    return cost;
+  };
+  int64_t padA = 0;
+  {
+    int64_t best = gather_cost(0);
+    for (int k = 1; k <= 8; ++k) {
+      int64_t cand = (int64_t)k * c.vecA;
+      if (cand > 32) break;
+      int64_t cc = gather_cost(cand);
+      if (cc < best) {
+        best = cc;
+        padA = cand;
+      }
+    }
+  }
+  const int64_t staged_size = staged(P - 1, padA) + 1;
+  std::vector<uint16_t> gtab(P);
+  for (int64_t q = 0; q < P; ++q) gtab[q] = (uint16_t)staged(p_of_q[q], padA);
   for (int64_t s = 0; s < nsegB; ++s) {
     int64_t rem = s * c.LB, offB = 0;
     for (int d : bord) {
@@ -414,15 +481,33 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   off = al16(off + 8 * nsegB);
   td.off_perm = (int32_t)off;
   off = al16(off + 2 * P);
+  td.off_gtab = (int32_t)off;
+  off = al16(off + 2 * P);
   int64_t smem = al16(phys_size * EA) + 8 * nsegA + 8 * nsegB + al16(2 * P);
   td.smem_bytes = (int32_t)smem;
+  {
+    // the fast kernel keeps tile-relative offsets in 32-bit registers
+    int64_t mA = 0, mB = 0;
+    for (int64_t x : segA) mA = std::max(mA, x + c.LA);
+    for (int64_t x : segB) mB = std::max(mB, x + c.LB);
+    td.fast = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && P / c.vecA <= 1024 && P / c.vecB <= 1024) ? 1 : 0;
+    td.padA = (int32_t)padA;
+    td.stage_elems = (int32_t)std::max<int64_t>(staged_size, phys_size);
+    const int64_t sb = al16(td.stage_elems * EA);
+    const int64_t tables = 8 * nsegA + 8 * nsegB + al16(2 * P);
+    td.nstages = (3 * sb + tables <= 80 * 1024) ? 3 : 2;
+    td.async_ok = (mA < (int64_t(1) << 31) && td.stage_elems < 65536 && td.nstages * sb + tables <= 200 * 1024) ? 1 : 0;
+    p->smem_async = (int)(td.nstages * sb + tables);
+  }
 
   p->host_desc.assign(off, 0);
   std::memcpy(p->host_desc.data(), &td, sizeof(td));
   std::memcpy(p->host_desc.data() + td.off_segA, segA.data(), 8 * nsegA);
   std::memcpy(p->host_desc.data() + td.off_segB, segB.data(), 8 * nsegB);
   std::memcpy(p->host_desc.data() + td.off_perm, ptab.data(), 2 * P);
+  std::memcpy(p->host_desc.data() + td.off_gtab, gtab.data(), 2 * P);
   p->smem_bytes = (int)smem;
+  p->smem_fast = (int)al16(phys_size * EA);
   p->vecA = c.vecA;
   p->vecB = c.vecB;
   p->est_cost = c.cost;
@@ -434,13 +519,13 @@ static ttcb_status build_row_desc(ttcb_plan* p, std::string& err) {
   RowDesc rd;
   std::memset(&rd, 0, sizeof(rd));
   rd.w = f.n[0];
-  int V = 16 / std::max(EA, EB);
   int64_t g = 0;
   for (int i = 1; i < f.rank; ++i) {
     g = gcd64(g, f.sA[i]);
     g = gcd64(g, f.sB[i]);
   }
-  if (V > 1 && !(g == 0 || g % V == 0)) V = 1;
+  int V = 16 / std::max(EA, EB);
+  while (V > 1 && !(g == 0 || g % V == 0)) V /= 2;
   if (p->tuning.vec == 1) V = 1;
   const int64_t chunk_max = 32 * V * 8;
   int64_t chunk = rd.w <= chunk_max ? rd.w : chunk_max;
@@ -578,7 +663,9 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
     if (row_possible) {
       double rb = (double)f.n[0] * std::max(EA, EB);
       double row_cost = (EA + (beta ? 2.0 : 1.0) * EB) / run_eff(rb, 16);
-      kernel = (!have_tile || rb >= 512 || row_cost <= best.cost * 1.05) ? TTCB_KERNEL_ROW : TTCB_KERNEL_TILE;
+      // short shared rows are slow to copy one warp per row; the tile kernel packs many of them
+      (void)row_cost;
+      kernel = (!have_tile || rb >= 512) ? TTCB_KERNEL_ROW : TTCB_KERNEL_TILE;
     } else {
       if (!have_tile) {
         err = "no tile shape fits this problem";
@@ -629,7 +716,8 @@ std::string plan_describe_json(const ttcb_plan* p) {
     const TileDesc* t = reinterpret_cast<const TileDesc*>(p->host_desc.data());
     o << ",\"tile\":{\"P\":" << t->P << ",\"LA\":" << t->LA << ",\"LB\":" << t->LB << ",\"ntiles\":" << t->ntiles
       << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
-      << ",\"pshift\":" << t->pshift << "}";
+      << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
+      << ",\"padA\":" << t->padA << ",\"stages\":" << t->nstages << "}";
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     o << ",\"row\":{\"w\":" << rd->w << ",\"chunk\":" << rd->chunk << ",\"units\":" << rd->nunits << "}";

@@ -41,7 +41,11 @@ struct ttcb_plan {
   // descriptor (host copy + device copy)
   std::vector<unsigned char> host_desc;
   void* dev_desc = nullptr;
-  int smem_bytes = 0;
+  int smem_bytes = 0;     // generic tile kernel (slots + tables)
+  int smem_fast = 0;      // fast tile kernel (slots only)
+  int blocks_fast = 0;    // CTAs for the fast tile kernel
+  int smem_async = 0;     // staged tile kernel (stages + tables)
+  int blocks_async = 0;   // CTAs for the staged tile kernel
   int device = 0;
 };
 
