@@ -93,6 +93,19 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
 ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const void* alpha,
                            const void* beta, ttcb_stream_t stream);
 
+/* Allocation-free transposition, for callers that may not allocate device memory (their memory is
+ * owned by an external pool, or cudaMalloc is forbidden where they run). It has no counterpart in
+ * TTC, whose every call allocates. Plans on the host and writes the plan's descriptor into a 64 KiB
+ * scratch array built into the library (held by every GPU that loads the library until exit);
+ * never calls cudaMalloc/cudaFree. Uses the staged tile kernel; beta == NULL means beta = 0.
+ * Problems whose descriptor exceeds the scratch size fail with TTCB_ERR_UNSUPPORTED. Calls that
+ * overlap on the GPU race on the scratch array; calls in order on one stream do not. The first call
+ * on each device looks up the scratch address and should come before any stream capture. */
+ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const int64_t* size, const int64_t* lda,
+                                   const int64_t* ldb, ttcb_dtype type_a, ttcb_dtype type_b,
+                                   const void* A, void* B, const void* alpha, const void* beta,
+                                   ttcb_stream_t stream);
+
 /* Frees the plan's device descriptor. Safe on NULL. */
 void ttcb_plan_destroy(ttcb_plan* plan);
 

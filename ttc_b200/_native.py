@@ -69,6 +69,8 @@ PUBLIC_SYMBOLS = [
     ("ttcb_batch_status", ctypes.c_int, [_P, _P]),
     ("ttcb_batch_bytes", ctypes.c_int64, [_P]),
     ("ttcb_batch_destroy", None, [_P]),
+    ("ttcb_transpose_noalloc", ctypes.c_int, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
+                                              _P, _P, _P, _P, _P]),
 ]
 
 TEST_SYMBOLS = [

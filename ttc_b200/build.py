@@ -30,7 +30,7 @@ def _units():
     units = []
     for i, name in enumerate(PAIRS):
         units.append((CSRC / "kernels_pair.cu", BUILD / f"kernels_{name}.o", [f"-DTTCB_PAIR={i}"]))
-    for src in ("abi.cu", "batched.cu"):
+    for src in ("abi.cu", "batched.cu", "noalloc.cu"):
         if (CSRC / src).exists():
             units.append((CSRC / src, BUILD / (Path(src).stem + ".o"), []))
     units.append((CSRC / "plan.cpp", BUILD / "plan.o", ["-x", "cu"]))
