@@ -56,6 +56,20 @@ def test_ttc_reference_case_matrix():
         check_case(perm, size, dtype, alpha, beta)
 
 
+def test_against_ttc_golden_fixtures():
+    """The GPU path against the outputs of TTC's own generated reference loop (tests/golden)."""
+    import json
+    from pathlib import Path
+    z = np.load(Path(__file__).resolve().parent / "golden" / "ttc_reference_loop.npz")
+    cases = json.loads(bytes(z["meta"]).decode())["cases"]
+    for k, c in enumerate(cases):
+        A, B = make_inputs(c["size"], c["perm"], c["dtype"], c["seed"], c["lda"], c["ldb"])
+        for tuning in (None, {"tile_variant": 1}, {"tile_variant": 2}):
+            got, desc = run_gpu(A, B, c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"], c["lda"], c["ldb"],
+                                tuning)
+            assert_bitexact(got, z[f"B{k}"], f"golden {k} {c} tuning={tuning} plan={desc}")
+
+
 def test_readme_shape_full_size():
     """perm 1,0,2 / 1000x768x16 fp32, alpha = beta = 1 (the README example)."""
     desc = check_case([1, 0, 2], [1000, 768, 16], "s", 1.0, 1.0)
