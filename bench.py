@@ -129,13 +129,16 @@ def ncu_traffic_per_gb(kernel: str):
 
 # ------------------------------------------------------------------------------------------------
 def cpu_prepare(cases):
-    """Seeded host inputs for the CPU baseline sample (untimed)."""
+    """Seeded host inputs for the CPU baseline sample (untimed), 64-byte aligned."""
+    from oracle.cpu_ref import aligned
     out = []
     for c in cases:
         real = np.float32 if c["dtype"] == "s" else np.float64
         na = math.prod(c["size"])
-        A = np.random.default_rng(c["seed"]).uniform(-1, 1, na).astype(real)
-        B = np.random.default_rng(c["seed"] + 1).uniform(-1, 1, na).astype(real)
+        A = aligned(na, real)
+        B = aligned(na, real)
+        A[:] = np.random.default_rng(c["seed"]).uniform(-1, 1, na)
+        B[:] = np.random.default_rng(c["seed"] + 1).uniform(-1, 1, na)
         out.append((c, A, B))
     return out
 

@@ -17,6 +17,15 @@ REF_DIR = Path(__file__).resolve().parent / "_ref"
 _cache = {}
 
 
+def aligned(n: int, dtype, align: int = 64) -> np.ndarray:
+    """A 1-D array whose data starts on an `align`-byte boundary. TTC's generated AVX code uses
+    aligned vector loads and stores (its default --align), so its buffers must be 32-byte aligned."""
+    dt = np.dtype(dtype)
+    raw = np.empty(n * dt.itemsize + align, dtype=np.uint8)
+    off = (-raw.ctypes.data) % align
+    return raw[off:off + n * dt.itemsize].view(dt)
+
+
 def manifest():
     f = REF_DIR / "manifest.json"
     if not f.exists():
@@ -39,6 +48,8 @@ def available():
     entries = {e["key"]: e for e in m["entries"]}
 
     def run(c, A: np.ndarray, B: np.ndarray, threads: int):
+        if A.ctypes.data % 32 or B.ctypes.data % 32:
+            raise ValueError("TTC's generated code needs 32-byte aligned buffers (use cpu_ref.aligned)")
         e = entries.get(_key(c))
         if e is None:
             raise KeyError(f"no generated TTC code for {_key(c)}")

@@ -1,9 +1,10 @@
-"""Loads modules of the TTC sources (Python 2) under Python 3, for generating golden fixtures.
+"""TEST INFRASTRUCTURE - loads modules of the TTC sources (Python 2) under Python 3.
 
 Copies the requested files from the TTC project into a scratch directory, expands tabs (the sources
 mix tabs and spaces), and rewrites the Python 2 constructs they use: print statements, integer `/`,
-`dict.has_key`, list-returning `range`, implicit relative imports. Only used by make_golden.py in
-this container; nothing at test time reads the TTC sources.
+`dict.has_key`, list-returning `range`, implicit relative imports, byte-string subprocess output.
+Used by tests/golden/make_golden.py and oracle/make_ref.py where the TTC sources exist; nothing at
+test or bench time reads the TTC sources.
 """
 from __future__ import annotations
 
@@ -84,6 +85,27 @@ def convert(src: str) -> str:
     src = _print_statements(src)
     tree = ast.fix_missing_locations(_Py2Semantics().visit(ast.parse(src)))
     return HELPER + ast.unparse(tree) + "\n"
+
+
+def convert_tree(src_dir: Path, dst_dir: Path, package_names: list[str]) -> None:
+    """Converts every module of a TTC checkout into dst_dir as a Python 3 package."""
+    dst_dir.mkdir(parents=True, exist_ok=True)
+    for f in src_dir.iterdir():
+        if f.is_dir():
+            shutil.copytree(f, dst_dir / f.name, dirs_exist_ok=True)
+        elif f.suffix != ".py":
+            shutil.copy(f, dst_dir / f.name)
+    for f in src_dir.glob("*.py"):
+        out = convert(f.read_text())
+        for other in package_names:
+            out = out.replace(f"\nimport {other} as ", f"\nfrom . import {other} as ")
+            out = out.replace(f"\nimport {other}\n", f"\nfrom . import {other}\n")
+        out = out.replace(".communicate()[0]", ".communicate()[0].decode()")
+        out = out.replace("proc = subprocess.Popen(['./transpose.exe'], stderr=subprocess.STDOUT, "
+                          "stdout=subprocess.PIPE, env=my_env)",
+                          "proc = subprocess.Popen(['./transpose.exe'], stderr=subprocess.STDOUT, "
+                          "stdout=subprocess.PIPE, env=my_env, text=True)")
+        (dst_dir / f.name).write_text(out)
 
 
 def load(ttc_dir: Path, names: list[str], package: str = "ttc_ref_py3"):

@@ -1,0 +1,109 @@
+"""TTC's driver surface on the host: argument parsing, names, index fusion, the generated shim (compiled
+with nvcc, not run), and the tuning database (round trip, corrupt file)."""
+import sqlite3
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import oracle.ttc_ref as ref
+from ttc_b200 import TTCError, sql_util, ttc, ttc_util
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_parse_args_matches_ttc_flags():
+    a = ttc.parse_args(["--perm=1,0,2", "--size=1000,768,16", "--beta=1.0", "--dataType=zc", "--alpha=0.5",
+                        "--lda=1000,770,16", "--maxImplementations=7", "--architecture=cuda", "--ignoreDatabase",
+                        "--blockings=32x32,64x64", "--loopPerm=0,1,2-2,1,0", "--threadsPerBlock=256", "--noTest"])
+    assert a.idxPerm == [1, 0, 2] and a.size == [1000, 768, 16]
+    assert (a.floatTypeA, a.floatTypeB) == ("double complex", "float complex")
+    assert a.alpha == 0.5 and a.beta == 1.0 and a.lda == [1000, 770, 16]
+    assert a.maxNumImplementations == 7 and a.ignoreDatabase == 1 and a.noTest == 1
+    assert a.blockings == [(32, 32), (64, 64)] and a.loopPermutations == [[0, 1, 2], [2, 1, 0]]
+    assert a.architecture == "cuda"
+    with pytest.raises(TTCError):
+        ttc.parse_args(["--perm=1,0", "--size=3,4", "--bogus=1"])
+    with pytest.raises(TTCError):
+        ttc.parse_args(["--perm=1,0", "--size=3,4,5"])
+    with pytest.raises(TTCError):
+        ttc.parse_args(["--perm=1,0", "--size=3,4", "--dataType=q"])
+    with pytest.raises(TTCError):
+        ttc.parse_args(["--perm=1,0", "--size=3,4", "--threadsPerBlock=100"])
+
+
+def test_transpose_names_follow_ttc():
+    a = ttc_util.TTCargs([1, 0, 2], [1000, 768, 16])
+    a.beta = 1.0
+    assert ttc.getTransposeName(a) == "sCuTranspose_102_1000x768x16"
+    a.beta = 0.0
+    assert ttc.getTransposeName(a) == "sCuTranspose_102_1000x768x16_bz"
+    a.floatTypeA, a.floatTypeB = "double complex", "float complex"
+    assert ttc.getTransposeName(a) == "zsCuTranspose_102_1000x768x16_bz"   # TTC's own spelling
+    assert ttc._function_name(a) == "zcCuTranspose_102_1000x768x16_bz"
+
+
+def test_fuse_indices_mirror_matches_reference_restatement():
+    import numpy as np
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        r = int(rng.integers(1, 6))
+        size = [int(x) for x in rng.integers(2, 6, r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        s1, p1, l1, b1 = list(size), list(perm), [], []
+        ttc_util.fuseIndices(s1, p1, [], l1, b1)
+        s2, p2, l2, b2 = ref.fuse_indices(size, perm)
+        assert (s1, p1, l1, b1) == (s2, p2, l2, b2)
+
+
+def test_cost_loop_mirror():
+    import numpy as np
+    rng = np.random.default_rng(6)
+    for _ in range(50):
+        r = int(rng.integers(2, 6))
+        size = [int(x) for x in rng.integers(2, 9, r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        lp = [int(x) for x in rng.permutation(r)]
+        assert ttc_util.getCostLoop(lp, perm, size) == ref.cost_loop(lp, perm, size)
+
+
+@pytest.mark.parametrize("dtype,beta", [("s", 1.0), ("zc", 0.0), ("cz", 2.0), ("ds", 0.0)])
+def test_generated_shim_compiles(tmp_path, dtype, beta):
+    a = ttc_util.TTCargs([2, 0, 1], [7, 8, 9])
+    a.floatTypeA, a.floatTypeB = ttc_util.TYPES_OF_PREFIX[dtype]
+    a.beta = beta
+    name = ttc.getTransposeName(a)
+    h, src = ttc.emit_shim(a, name, ttc._function_name(a), {"tile_elems": 1024, "loop_order": 1}, [7, 8, 9],
+                           [2, 0, 1], None, None)
+    (tmp_path / f"{name}.h").write_text(h)
+    (tmp_path / f"{name}.cu").write_text(src)
+    r = subprocess.run(["/usr/local/cuda/bin/nvcc", "-c", "-I", str(ROOT / "include"), "-o", str(tmp_path / "x.o"),
+                        str(tmp_path / f"{name}.cu")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    nm = subprocess.run(["nm", str(tmp_path / "x.o")], capture_output=True, text=True).stdout
+    assert ttc._function_name(a) in nm and name in nm
+
+
+def test_database_round_trip_and_corrupt_file(tmp_path):
+    db = str(tmp_path / "ttc.db")
+    variants = [{"tuning": {"tile_elems": 1024}, "bandwidth": 10.0, "time": 1e-3, "rank": 1},
+                {"tuning": {"run_bytes": 256}, "bandwidth": 20.0, "time": 5e-4, "rank": 0}]
+    sql_util.insert(db, [1000, 768, 16], [1, 0, 2], "float", "float", 1.0, 1.0, " NVIDIA B200", "h", variants, 1.0)
+    hit = sql_util.lookup(db, [1000, 768, 16], [1, 0, 2], "float", "float", 1.0, " NVIDIA B200")
+    assert hit["tuning"] == {"run_bytes": 256} and hit["bandwidth"] == 20.0
+    assert sql_util.lookup(db, [1000, 768, 16], [1, 0, 2], "float", "float", 0.0, " NVIDIA B200") is None
+    assert sql_util.lookup(db, [1000, 768, 16], [1, 0, 2], "double", "double", 1.0, " NVIDIA B200") is None
+    con = sqlite3.connect(db)
+    rows = con.execute("SELECT * FROM fastest0Percent").fetchall()
+    assert len(rows) == 1
+    con.close()
+    bad = tmp_path / "bad.db"
+    bad.write_bytes(b"this is not a database" * 100)
+    with pytest.raises(sql_util.DatabaseUnavailable):
+        sql_util.lookup(str(bad), [4, 4], [1, 0], "float", "float", 0.0, "x")
+
+
+def test_main_reports_errors_without_exiting(capsys):
+    assert ttc.main(["--perm=1,0", "--size=3,4", "--lda=2,4", "--architecture=cuda"]) == 1
+    out = capsys.readouterr().out
+    assert "leading dimension of A" in out

@@ -1,0 +1,204 @@
+"""Measured search over the schedule space, the counterpart of TTC's exhaustive variant timing
+(ttc.py:847-1022, GPUtransposeGenerator.py:165-230 in the TTC project).
+
+TTC generates every (blocking x loop order) variant as source, compiles them all and times each
+with wall-clock around the wrapper. Here a candidate is a `ttcb_tuning` (tile size target, run
+length target, tile kernel variant, grid raster order, CTA count): the planner turns it into a plan
+in microseconds, so the search costs only kernel time. Candidates are deduplicated by the plan they
+produce, ordered by the planner's cost estimate and capped at maxImplementations, like TTC's
+pruning. Every candidate's output is compared with the first candidate's (all schedules must agree
+bit for bit); timing uses CUDA events around each launch with the L2 flushed in between, minimum
+over repetitions.
+"""
+from __future__ import annotations
+
+import itertools
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+from .core import ELEM_BYTES, Plan, plan_host_json, split_dtype
+
+SMS = 148
+L2_BYTES = 126 * 1024 * 1024
+
+
+@dataclass
+class Problem:
+    perm: list
+    size: list
+    dtype: str = "s"
+    alpha: complex | float = 1.0
+    beta: complex | float = 0.0
+    lda: Optional[list] = None
+    ldb: Optional[list] = None
+
+    @property
+    def beta_nonzero(self) -> bool:
+        return complex(self.beta) != 0
+
+    def elements(self) -> int:
+        return math.prod(self.size)
+
+    def bytes(self) -> int:
+        ta, tb = split_dtype(self.dtype)
+        return self.elements() * (ELEM_BYTES[ta] + ELEM_BYTES[tb] * (2 if self.beta_nonzero else 1))
+
+    def buffer_elems(self):
+        la = self.lda or self.size
+        lb = self.ldb or [self.size[p] for p in self.perm]
+        na = math.prod(la[:-1]) * self.size[-1]
+        nb = math.prod(lb[:-1]) * self.size[self.perm[-1]]
+        return max(na, 1), max(nb, 1)
+
+
+@dataclass
+class Result:
+    tuning: dict
+    time_ms: float
+    gbs: float
+    desc: dict = field(default_factory=dict)
+    ok: bool = True
+
+
+def knob_space(dtype: str) -> dict:
+    ta, _ = split_dtype(dtype)
+    base = 16384 // ELEM_BYTES[ta]
+    return {
+        "tile_elems": [0, base // 4, base // 2, base * 2],
+        "run_bytes": [0, 128, 256, 512, 1024, 2048],
+        "tile_variant": [0, 2, 1],
+        "loop_order": [0, 1, 2],
+        "blocks": [0, 2 * SMS, 3 * SMS],
+    }
+
+
+def plan_signature(desc: dict) -> tuple:
+    t = desc.get("tile") or desc.get("row") or {}
+    return (desc["kernel"], desc["vecA"], desc["vecB"], t.get("P", t.get("w")), t.get("LA"), t.get("LB"),
+            t.get("ntiles", t.get("units")))
+
+
+def tile_shapes(p: Problem, space: Optional[dict] = None) -> list[tuple[dict, dict]]:
+    """Distinct plans the shape knobs (tile_elems x run_bytes) produce: [(shape knobs, plan json)]."""
+    space = space or knob_space(p.dtype)
+    seen = {}
+    for te, rb in itertools.product(space["tile_elems"], space["run_bytes"]):
+        tu = {k: v for k, v in (("tile_elems", te), ("run_bytes", rb)) if v}
+        try:
+            desc = plan_host_json(p.perm, p.size, p.dtype, p.beta_nonzero, p.lda, p.ldb, tu or None)
+        except Exception:
+            continue
+        sig = plan_signature(desc)
+        if sig not in seen:
+            seen[sig] = (tu, desc)
+    return sorted(seen.values(), key=lambda x: (x[1]["est_cost"], len(x[0])))
+
+
+def candidate_tunings(p: Problem, max_impl: int = 200, space: Optional[dict] = None,
+                      with_desc: bool = False) -> list:
+    """Distinct schedules for a problem, at most max_impl. The grid raster order, CTA count and tile
+    kernel variant do not change the tile, so only the shape knobs are planned on the host.
+
+    TTC keeps the best sqrt(maxImpl) blockings x sqrt(maxImpl) loop orders
+    (GPUtransposeGenerator.py:220-230); here the tile shapes are ordered by the planner's estimate
+    and taken round-robin, so every shape gets its default schedule before any gets a second one."""
+    space = space or knob_space(p.dtype)
+    lists = []
+    for shape_tu, desc in tile_shapes(p, space):
+        if desc["kernel"] == "row":
+            combos = [dict(shape_tu, blocks=b) if b else dict(shape_tu) for b in space["blocks"]]
+        else:
+            combos = []
+            for v, lo, b in itertools.product(space["tile_variant"], space["loop_order"], space["blocks"]):
+                tu = dict(shape_tu)
+                for k, val in (("tile_variant", v), ("loop_order", lo), ("blocks", b)):
+                    if val:
+                        tu[k] = val
+                combos.append(tu)
+        lists.append([(tu, desc) for tu in combos])
+    out = []
+    depth = 0
+    while len(out) < max(1, max_impl) and any(depth < len(l) for l in lists):
+        for l in lists:
+            if depth < len(l) and len(out) < max(1, max_impl):
+                out.append(l[depth])
+        depth += 1
+    return out if with_desc else [tu for tu, _ in out]
+
+
+class Bench:
+    """Device buffers for timing one problem's candidates (allocated once per problem)."""
+
+    def __init__(self, p: Problem, seed: int = 0):
+        import torch
+        self.p = p
+        ta, tb = split_dtype(p.dtype)
+        tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
+        na, nb = p.buffer_elems()
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        self.A = torch.rand(na, dtype=tmap[ta], device="cuda", generator=g)
+        self.B0 = torch.rand(nb, dtype=tmap[tb], device="cuda", generator=g)
+        self.B = self.B0.clone()
+        self.ref = None
+        self.flush_buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def flush(self):
+        self.flush_buf.zero_()
+
+    def run_once(self, plan: Plan):
+        self.B.copy_(self.B0)
+        plan(self.A, self.B, self.p.alpha, self.p.beta)
+
+    def time(self, plan: Plan, reps: int = 5, warmup: int = 1) -> float:
+        import torch
+        for _ in range(warmup):
+            plan(self.A, self.B, self.p.alpha, self.p.beta)
+        best = float("inf")
+        small = self.p.bytes() < 2 * L2_BYTES
+        for _ in range(reps):
+            if small:
+                self.flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan(self.A, self.B, self.p.alpha, self.p.beta)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+
+def measure(p: Problem, tunings: Sequence[dict], reps: int = 5, verify: bool = True, seed: int = 0,
+            bench: Optional[Bench] = None) -> list[Result]:
+    """Times every tuning on one problem; with verify, checks each output against the first."""
+    import torch
+    bench = bench or Bench(p, seed)
+    out = []
+    for tu in tunings:
+        plan = Plan(p.perm, p.size, p.dtype, p.beta_nonzero, p.lda, p.ldb, tu or None)
+        ok = True
+        if verify:
+            bench.run_once(plan)
+            if bench.ref is None:
+                bench.ref = bench.B.clone()
+            else:
+                ok = bool(torch.equal(bench.B.view(torch.uint8), bench.ref.view(torch.uint8)))
+        ms = bench.time(plan, reps)
+        out.append(Result(dict(tu), ms, p.bytes() / (ms * 1e-3) / 1e9, plan.describe(), ok))
+        plan.close()
+    return out
+
+
+def search(p: Problem, max_impl: int = 200, reps: int = 5, verify: bool = True, seed: int = 0) -> dict:
+    """Exhaustive measured search. Returns {'best': Result, 'results': [...], 'seconds': wall}."""
+    t0 = time.perf_counter()
+    cands = candidate_tunings(p, max_impl)
+    res = measure(p, cands, reps, verify, seed)
+    bad = [r for r in res if not r.ok]
+    if bad:
+        raise RuntimeError(f"[TTC] ERROR: {len(bad)} schedules disagree with the first one: {bad[0].tuning}")
+    best = min(res, key=lambda r: r.time_ms)
+    return {"best": best, "results": res, "seconds": time.perf_counter() - t0, "candidates": len(cands)}

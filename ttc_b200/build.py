@@ -30,7 +30,7 @@ def _units():
     units = []
     for i, name in enumerate(PAIRS):
         units.append((CSRC / "kernels_pair.cu", BUILD / f"kernels_{name}.o", [f"-DTTCB_PAIR={i}"]))
-    for src in ("abi.cu", "batched.cu", "noalloc.cu"):
+    for src in ("abi.cu", "batched.cu", "noalloc.cu", "mlp.cu"):
         if (CSRC / src).exists():
             units.append((CSRC / src, BUILD / (Path(src).stem + ".o"), []))
     units.append((CSRC / "plan.cpp", BUILD / "plan.o", ["-x", "cu"]))
@@ -43,7 +43,8 @@ def _fingerprint(extra: list[str]) -> str:
         if p.suffix in (".cu", ".cuh", ".h", ".cpp"):
             h.update(p.name.encode())
             h.update(p.read_bytes())
-    h.update((ROOT / "include" / "ttcb200.h").read_bytes())
+    for hdr in sorted((ROOT / "include").glob("*.h")):
+        h.update(hdr.read_bytes())
     h.update(" ".join(ARCH + COMMON + extra).encode())
     return h.hexdigest()
 

@@ -1,0 +1,471 @@
+"""Learned schedule selection: an MLP that ranks the autotuner's candidate schedules.
+
+TTC picks a transposition's variant by compiling and timing every candidate (ttc.py:847-1022,
+GPUtransposeGenerator.py:165-230). Here a 3-layer fp32 MLP (128 hidden units) predicts log(GB/s)
+of every candidate schedule from problem and schedule features; the top prediction is used directly
+when the model is confident, otherwise the top-k predictions are measured (a short measured search).
+
+Features: rank, the permutation as one-hot, log2 extents, log2 strides of A and B, element sizes,
+beta != 0, and the candidate's tile (size, run lengths), access widths, tile kernel variant, grid
+raster order and CTA count, plus the planner's own cost estimate.
+
+The network is trained on the GPU with the library's own kernels (include/ttcb200_mlp.h: tiled GEMM
+with fused bias/ReLU, ReLU backward, column sums, MSE, Adam) on timings the measured search itself
+produced (`collect`). `python -m ttc_b200.cost_model collect|train|evaluate ...` runs each step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import hashlib
+import json
+import math
+import time
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import _native
+from .autotune import Problem, candidate_tunings, measure, Bench
+from .core import ELEM_BYTES, split_dtype
+
+MAXD = 6
+DEFAULT_MODEL = Path(__file__).resolve().parent / "data" / "cost_model.npz"
+VERSION = "ttcb-mlp-v1"
+
+
+# ------------------------------------------------------------------------------------------------
+def problem_features(p: Problem, desc: dict) -> list[float]:
+    r = len(p.size)
+    f = [r / MAXD]
+    onehot = [0.0] * (MAXD * MAXD)
+    for j, d in enumerate(p.perm[:MAXD]):
+        if d < MAXD:
+            onehot[j * MAXD + d] = 1.0
+    f += onehot
+    ext = [math.log2(max(s, 1)) / 20.0 for s in p.size[:MAXD]]
+    f += ext + [0.0] * (MAXD - len(ext))
+    la = p.lda or p.size
+    lb = p.ldb or [p.size[q] for q in p.perm]
+    sA = [1] * r
+    sBp = [1] * r
+    for i in range(1, r):
+        sA[i] = sA[i - 1] * la[i - 1]
+        sBp[i] = sBp[i - 1] * lb[i - 1]
+    sB = [0] * r
+    for j, q in enumerate(p.perm):
+        sB[q] = sBp[j]
+    ls = [math.log2(max(x, 1)) / 30.0 for x in sA[:MAXD]]
+    f += ls + [0.0] * (MAXD - len(ls))
+    ls = [math.log2(max(x, 1)) / 30.0 for x in sB[:MAXD]]
+    f += ls + [0.0] * (MAXD - len(ls))
+    ta, tb = split_dtype(p.dtype)
+    f += [ELEM_BYTES[ta] / 16.0, ELEM_BYTES[tb] / 16.0, 1.0 if p.beta_nonzero else 0.0,
+          math.log2(max(p.elements(), 1)) / 30.0]
+    fu = desc["fused"]
+    f += [fu["rank"] / MAXD, 1.0 if fu["perm"] and fu["perm"][0] == 0 else 0.0]
+    return f
+
+
+def candidate_features(p: Problem, tuning: dict, desc: dict) -> list[float]:
+    ta, tb = split_dtype(p.dtype)
+    t = desc.get("tile") or {}
+    row = desc.get("row") or {}
+    is_tile = desc["kernel"] == "tile"
+    P = t.get("P", row.get("chunk", 1))
+    LA = t.get("LA", row.get("w", 1))
+    LB = t.get("LB", row.get("w", 1))
+    nt = t.get("ntiles", row.get("units", 1))
+    tv = tuning.get("tile_variant", 0)
+    lo = tuning.get("loop_order", 0)
+    bl = tuning.get("blocks", 0)
+    f = [1.0 if is_tile else 0.0, 0.0 if is_tile else 1.0,
+         math.log2(max(P, 1)) / 14.0, math.log2(max(LA, 1)) / 14.0, math.log2(max(LB, 1)) / 14.0,
+         desc["vecA"] / 4.0, desc["vecB"] / 4.0,
+         math.log2(max(LA * ELEM_BYTES[ta], 1)) / 16.0, math.log2(max(LB * ELEM_BYTES[tb], 1)) / 16.0,
+         1.0 if tv == 0 else 0.0, 1.0 if tv == 2 else 0.0, 1.0 if tv == 1 else 0.0,
+         1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
+         1.0 if bl == 0 else 0.0, bl / 444.0,
+         min(desc["est_cost"], 200.0) / 32.0, math.log2(max(nt, 1)) / 25.0,
+         float(t.get("fast", 0)), float(t.get("async", 0)), float(t.get("stages", 0)) / 3.0]
+    return f
+
+
+def features(p: Problem, cands) -> np.ndarray:
+    """Feature matrix for [(tuning, plan json)] candidates of one problem."""
+    if not cands:
+        return np.zeros((0, 0), np.float32)
+    pf = problem_features(p, cands[0][1])
+    return np.asarray([pf + candidate_features(p, tu, d) for tu, d in cands], dtype=np.float32)
+
+
+# ------------------------------------------------------------------------------------------------
+def _lib():
+    lib = _native.lib()
+    if not hasattr(lib, "_mlp_bound"):
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        F = ctypes.c_float
+        lib.ttcb_mlp_gemm.argtypes = [I, I, I, I, I, P, I, P, I, P, I, P, I, P]
+        lib.ttcb_mlp_relu_grad.argtypes = [P, P, P, I, P]
+        lib.ttcb_mlp_colsum.argtypes = [P, I, I, P, P]
+        lib.ttcb_mlp_mse.argtypes = [P, P, I, P, P, P]
+        lib.ttcb_mlp_adam.argtypes = [P, P, P, P, I, F, F, F, F, I, P]
+        for n in ("ttcb_mlp_gemm", "ttcb_mlp_relu_grad", "ttcb_mlp_colsum", "ttcb_mlp_mse", "ttcb_mlp_adam"):
+            getattr(lib, n).restype = ctypes.c_int
+        lib._mlp_bound = True
+    return lib
+
+
+def _s():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def gemm(A, B, transA=False, transB=False, bias=None, relu=False, out=None):
+    """op(A) @ op(B) (+bias) (relu) with the library's kernel; torch tensors hold the memory."""
+    import torch
+    M = A.shape[1] if transA else A.shape[0]
+    K = A.shape[0] if transA else A.shape[1]
+    N = B.shape[0] if transB else B.shape[1]
+    C = out if out is not None else torch.empty((M, N), dtype=torch.float32, device=A.device)
+    _native.check(_lib().ttcb_mlp_gemm(int(transA), int(transB), M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(),
+                                       B.shape[1], C.data_ptr(), N, bias.data_ptr() if bias is not None else None,
+                                       int(relu), _s()))
+    return C
+
+
+class MLP:
+    """Three dense layers (nin -> h -> h -> 1), ReLU between them, fp32 on the GPU."""
+
+    def __init__(self, nin: int, hidden: int = 128, seed: int = 0):
+        import torch
+        g = np.random.default_rng(seed)
+
+        def init(i, o):
+            return torch.from_numpy((g.standard_normal((i, o)) * math.sqrt(2.0 / i)).astype(np.float32)).cuda()
+
+        self.nin, self.hidden = nin, hidden
+        self.params = [init(nin, hidden), torch.zeros(hidden, device="cuda"),
+                       init(hidden, hidden), torch.zeros(hidden, device="cuda"),
+                       init(hidden, 1) * 0.1, torch.zeros(1, device="cuda")]
+        self.m = [torch.zeros_like(p) for p in self.params]
+        self.v = [torch.zeros_like(p) for p in self.params]
+        self.t = 0
+        self.mu = np.zeros(nin, np.float32)
+        self.sd = np.ones(nin, np.float32)
+        self.ymu, self.ysd = 0.0, 1.0
+        self.rmse = 1.0
+
+    def forward(self, X):
+        W1, b1, W2, b2, W3, b3 = self.params
+        H1 = gemm(X, W1, bias=b1, relu=True)
+        H2 = gemm(H1, W2, bias=b2, relu=True)
+        out = gemm(H2, W3, bias=b3)
+        return out, (X, H1, H2)
+
+    def backward(self, dout, cache):
+        import torch
+        X, H1, H2 = cache
+        W1, b1, W2, b2, W3, b3 = self.params
+        lib, s = _lib(), _s()
+        grads = [None] * 6
+        grads[4] = gemm(H2, dout, transA=True)
+        grads[5] = torch.empty(1, device="cuda")
+        _native.check(lib.ttcb_mlp_colsum(dout.data_ptr(), dout.shape[0], 1, grads[5].data_ptr(), s))
+        dH2 = gemm(dout, W3, transB=True)
+        dZ2 = torch.empty_like(dH2)
+        _native.check(lib.ttcb_mlp_relu_grad(H2.data_ptr(), dH2.data_ptr(), dZ2.data_ptr(), dH2.numel(), s))
+        grads[2] = gemm(H1, dZ2, transA=True)
+        grads[3] = torch.empty(self.hidden, device="cuda")
+        _native.check(lib.ttcb_mlp_colsum(dZ2.data_ptr(), dZ2.shape[0], dZ2.shape[1], grads[3].data_ptr(), s))
+        dH1 = gemm(dZ2, W2, transB=True)
+        dZ1 = torch.empty_like(dH1)
+        _native.check(lib.ttcb_mlp_relu_grad(H1.data_ptr(), dH1.data_ptr(), dZ1.data_ptr(), dH1.numel(), s))
+        grads[0] = gemm(X, dZ1, transA=True)
+        grads[1] = torch.empty(self.hidden, device="cuda")
+        _native.check(lib.ttcb_mlp_colsum(dZ1.data_ptr(), dZ1.shape[0], dZ1.shape[1], grads[1].data_ptr(), s))
+        return grads
+
+    def loss_grad(self, out, y):
+        import torch
+        d = torch.empty_like(out)
+        loss = torch.zeros(1, device="cuda")
+        _native.check(_lib().ttcb_mlp_mse(out.data_ptr(), y.data_ptr(), out.numel(), d.data_ptr(), loss.data_ptr(),
+                                          _s()))
+        return loss, d
+
+    def step(self, grads, lr=1e-3):
+        self.t += 1
+        lib, s = _lib(), _s()
+        for p, g, m, v in zip(self.params, grads, self.m, self.v):
+            _native.check(lib.ttcb_mlp_adam(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(), lr,
+                                            0.9, 0.999, 1e-8, self.t, s))
+
+    # -- normalisation and I/O ------------------------------------------------------------------
+    def _norm(self, X: np.ndarray):
+        import torch
+        return torch.from_numpy(((X - self.mu) / self.sd).astype(np.float32)).cuda()
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        """Predicted log(GB/s) for each row of X."""
+        out, _ = self.forward(self._norm(X))
+        return out.reshape(-1).cpu().numpy() * self.ysd + self.ymu
+
+    def save(self, path: Path, extra: Optional[dict] = None):
+        path.parent.mkdir(parents=True, exist_ok=True)
+        arrays = {f"p{i}": p.cpu().numpy() for i, p in enumerate(self.params)}
+        meta = {"version": VERSION, "nin": self.nin, "hidden": self.hidden, "ymu": self.ymu, "ysd": self.ysd,
+                "rmse": self.rmse}
+        meta.update(extra or {})
+        np.savez(path, mu=self.mu, sd=self.sd, meta=np.frombuffer(json.dumps(meta).encode(), np.uint8), **arrays)
+
+    @classmethod
+    def load(cls, path: Path) -> "MLP":
+        import torch
+        z = np.load(path)
+        meta = json.loads(bytes(z["meta"]).decode())
+        if meta.get("version") != VERSION:
+            raise ValueError(f"cost model {path} has version {meta.get('version')}, expected {VERSION}")
+        m = cls(meta["nin"], meta["hidden"])
+        m.params = [torch.from_numpy(z[f"p{i}"]).cuda() for i in range(6)]
+        m.mu, m.sd = z["mu"], z["sd"]
+        m.ymu, m.ysd, m.rmse = meta["ymu"], meta["ysd"], meta["rmse"]
+        m.meta = meta
+        return m
+
+
+def numpy_forward_backward(params, X, y):
+    """CPU restatement (float64) of the same network's loss and gradients, for gradient checks."""
+    W1, b1, W2, b2, W3, b3 = [np.asarray(p, np.float64) for p in params]
+    X = np.asarray(X, np.float64)
+    y = np.asarray(y, np.float64).reshape(-1, 1)
+    Z1 = X @ W1 + b1
+    H1 = np.maximum(Z1, 0)
+    Z2 = H1 @ W2 + b2
+    H2 = np.maximum(Z2, 0)
+    out = H2 @ W3 + b3
+    n = out.size
+    loss = float(np.mean((out - y) ** 2))
+    d = 2 * (out - y) / n
+    gW3 = H2.T @ d
+    gb3 = d.sum(0)
+    dH2 = d @ W3.T
+    dZ2 = dH2 * (Z2 > 0)
+    gW2 = H1.T @ dZ2
+    gb2 = dZ2.sum(0)
+    dH1 = dZ2 @ W2.T
+    dZ1 = dH1 * (Z1 > 0)
+    gW1 = X.T @ dZ1
+    gb1 = dZ1.sum(0)
+    return loss, [gW1, gb1, gW2, gb2, gW3, gb3]
+
+
+def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batch: int = 2048, seed: int = 0,
+          val: float = 0.1, log=print) -> MLP:
+    """Fits log(GB/s) with the library's kernels; holds out `val` of the problems' rows for RMSE."""
+    import torch
+    rng = np.random.default_rng(seed)
+    idx = rng.permutation(len(X))
+    nval = int(len(X) * val)
+    vi, ti = idx[:nval], idx[nval:]
+    m = MLP(X.shape[1], 128, seed)
+    m.mu = X[ti].mean(0)
+    m.sd = X[ti].std(0) + 1e-6
+    m.ymu, m.ysd = float(y[ti].mean()), float(y[ti].std() + 1e-6)
+    Xt = m._norm(X[ti])
+    yt = torch.from_numpy(((y[ti] - m.ymu) / m.ysd).astype(np.float32)).cuda().reshape(-1, 1)
+    for ep in range(epochs):
+        order = torch.from_numpy(rng.permutation(len(ti))).cuda()
+        tot = 0.0
+        for b0 in range(0, len(ti), batch):
+            sel = order[b0:b0 + batch]
+            xb, yb = Xt[sel].contiguous(), yt[sel].contiguous()
+            out, cache = m.forward(xb)
+            loss, d = m.loss_grad(out, yb)
+            grads = m.backward(d, cache)
+            m.step(grads, lr * (0.5 ** (ep // 20)))
+            tot += float(loss.item()) * len(sel)
+        if log and (ep % 10 == 0 or ep == epochs - 1):
+            vr = np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)) if nval else float("nan")
+            log(f"epoch {ep}: train mse {tot / len(ti):.4f} (normalised), val rmse {vr:.4f} log(GB/s)")
+    if nval:
+        m.rmse = float(np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)))
+    return m
+
+
+# ------------------------------------------------------------------------------------------------
+def confidence_of(pred: np.ndarray, rmse: float) -> float:
+    """1 - exp(-gap / rmse): gap = predicted log-GB/s margin of the best over the second-best."""
+    if len(pred) < 2:
+        return 1.0
+    top = np.sort(pred)[::-1]
+    return float(1.0 - math.exp(-(top[0] - top[1]) / max(rmse, 1e-6)))
+
+
+_loaded = {}
+
+
+def load_default(path: Optional[Path] = None) -> MLP:
+    path = Path(path or DEFAULT_MODEL)
+    if str(path) not in _loaded:
+        _loaded[str(path)] = MLP.load(path)
+    return _loaded[str(path)]
+
+
+def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, verify: bool = True,
+           model: Optional[MLP] = None, topk: int = 8, measure_choice: bool = True) -> dict:
+    """Picks a schedule with the model. Below the confidence threshold, measures the top-k
+    predictions and keeps the fastest (a short measured search). Returns the measured results."""
+    model = model or load_default()
+    thr = 0.35 if confidence is None else confidence
+    t0 = time.perf_counter()
+    cands = candidate_tunings(p, max_impl, with_desc=True)
+    X = features(p, cands)
+    pred = model.predict(X)
+    order = np.argsort(-pred)
+    conf = confidence_of(pred, model.rmse)
+    fallback = conf < thr
+    chosen = [cands[i][0] for i in order[: (topk if fallback else 1)]]
+    t_model = time.perf_counter() - t0
+    results = measure(p, chosen, reps=3, verify=verify) if (measure_choice or fallback) else []
+    return {"results": results, "confidence": conf, "fallback": fallback, "pred": pred, "order": order,
+            "candidates": cands, "seconds_model": t_model, "seconds": time.perf_counter() - t0}
+
+
+# ------------------------------------------------------------------------------------------------
+def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log=print) -> None:
+    """Exhaustive measured search over each case's candidates; stores features, log(GB/s), the
+    search wall time, resumable per case (rows of finished cases are kept)."""
+    import torch
+    done = {}
+    if out.exists():
+        z = np.load(out, allow_pickle=False)
+        done = {"X": list(z["X"]), "y": list(z["y"]), "case": list(z["case"]), "cand": list(z["cand"]),
+                "search_s": list(z["search_s"]), "meta": json.loads(bytes(z["meta"]).decode())}
+    else:
+        done = {"X": [], "y": [], "case": [], "cand": [], "search_s": [], "meta": {"cases": [], "tunings": []}}
+    finished = {int(c) for c in done["case"]}
+    t_last = time.time()
+    for k, c in enumerate(cases):
+        if k in finished:
+            continue
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        t0 = time.perf_counter()
+        cands = candidate_tunings(p, max_impl, with_desc=True)
+        res = measure(p, [tu for tu, _ in cands], reps=reps, verify=True, seed=k)
+        secs = time.perf_counter() - t0
+        if not all(r.ok for r in res):
+            raise RuntimeError(f"schedules disagree on case {k}: {c}")
+        X = features(p, cands)
+        for j, r in enumerate(res):
+            done["X"].append(X[j])
+            done["y"].append(math.log(max(r.gbs, 1e-3)))
+            done["case"].append(k)
+            done["cand"].append(j)
+        done["search_s"].append(secs)
+        done["meta"]["cases"].append(dict(c, index=k))
+        done["meta"]["tunings"].append([tu for tu, _ in cands])
+        torch.cuda.empty_cache()
+        if time.time() - t_last > 60 or k == len(cases) - 1:
+            _save_corpus(out, done)
+            t_last = time.time()
+            if log:
+                log(f"collected {k + 1}/{len(cases)} cases, {len(done['y'])} rows")
+    _save_corpus(out, done)
+
+
+def _save_corpus(out: Path, d: dict):
+    out.parent.mkdir(parents=True, exist_ok=True)
+    np.savez(out, X=np.asarray(d["X"], np.float32), y=np.asarray(d["y"], np.float32),
+             case=np.asarray(d["case"], np.int32), cand=np.asarray(d["cand"], np.int32),
+             search_s=np.asarray(d["search_s"], np.float64),
+             meta=np.frombuffer(json.dumps(d["meta"]).encode(), np.uint8))
+
+
+def evaluate(model: MLP, corpus: Path, log=print, threshold: float = 0.35, topk: int = 8,
+             time_cases: int = 100) -> dict:
+    """Held-out evaluation from stored exhaustive measurements: model top-1 (or top-k when not
+    confident) GB/s vs the best measured, and the planner default (no model) vs the best. Model
+    selection time is measured on the first `time_cases` problems (candidate planning + features +
+    inference, plus the top-k measurements when it falls back)."""
+    z = np.load(corpus)
+    X, y, case = z["X"], z["y"], z["case"]
+    meta = json.loads(bytes(z["meta"]).decode())
+    search_s = z["search_s"]
+    ratios, default_ratios, fallbacks = [], [], 0
+    pred = model.predict(X)
+    index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
+    for k in np.unique(case):
+        rows = np.nonzero(case == k)[0]
+        tunings = meta["tunings"][index_of[int(k)]]
+        dflt = tunings.index({}) if {} in tunings else 0
+        best = np.exp(y[rows].max())
+        pk = pred[rows]
+        conf = confidence_of(pk, model.rmse)
+        if conf < threshold:
+            fallbacks += 1
+            top = rows[np.argsort(-pk)[:topk]]
+            chosen = np.exp(y[top].max())
+        else:
+            chosen = np.exp(y[rows[np.argmax(pk)]])
+        ratios.append(chosen / best)
+        default_ratios.append(np.exp(y[rows[dflt]]) / best)  # the planner's default schedule
+    ratios = np.asarray(ratios)
+    default_ratios = np.asarray(default_ratios)
+    # selection time on real problems
+    t_sel, t_search = [], []
+    cases = meta["cases"]
+    for i, c in enumerate(cases[:time_cases]):
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        r = select(p, confidence=threshold, model=model, topk=topk, verify=False, measure_choice=False)
+        t_sel.append(r["seconds"])
+        t_search.append(search_s[i])
+    res = {"cases": int(len(ratios)), "model_over_best_mean": float(ratios.mean()),
+           "model_over_best_median": float(np.median(ratios)), "model_within_5pct": float(np.mean(ratios >= 0.95)),
+           "default_over_best_mean": float(default_ratios.mean()),
+           "default_within_5pct": float(np.mean(default_ratios >= 0.95)),
+           "gain_over_default_mean": float(np.mean(ratios / default_ratios)),
+           "fallback_fraction": fallbacks / max(1, len(ratios)),
+           "search_seconds_mean": float(np.mean(t_search)), "model_seconds_mean": float(np.mean(t_sel)),
+           "tuning_time_ratio": float(np.mean(t_search) / max(np.mean(t_sel), 1e-9)),
+           "threshold": threshold, "topk": topk, "rmse": model.rmse}
+    if log:
+        log(json.dumps(res, indent=1))
+    return res
+
+
+def main(argv=None):
+    import ttc_b200.workloads as wl
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["collect", "train", "evaluate"])
+    ap.add_argument("--train-cases", type=int, default=2000)
+    ap.add_argument("--test-cases", type=int, default=500)
+    ap.add_argument("--corpus", default="gpurun_out/cost_corpus")
+    ap.add_argument("--model", default=str(DEFAULT_MODEL))
+    ap.add_argument("--max-impl", type=int, default=64)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--threshold", type=float, default=0.35)
+    ap.add_argument("--out-json", default=None)
+    a = ap.parse_args(argv)
+    train_path = Path(a.corpus + "_train.npz")
+    test_path = Path(a.corpus + "_test.npz")
+    if a.cmd == "collect":
+        collect(wl.learning_cases(11, a.train_cases), train_path, a.max_impl)
+        collect(wl.learning_cases(12345, a.test_cases), test_path, a.max_impl)
+    elif a.cmd == "train":
+        z = np.load(train_path)
+        m = train(z["X"], z["y"], epochs=a.epochs)
+        digest = hashlib.sha256(z["X"].tobytes()[:1 << 20]).hexdigest()[:16]
+        m.save(Path(a.model), {"trained_rows": int(len(z["y"])), "corpus_digest": digest})
+        print(f"saved {a.model} (val rmse {m.rmse:.4f})")
+    else:
+        m = MLP.load(Path(a.model))
+        res = evaluate(m, test_path, threshold=a.threshold)
+        if a.out_json:
+            Path(a.out_json).write_text(json.dumps(res, indent=1))
+
+
+if __name__ == "__main__":
+    main()
