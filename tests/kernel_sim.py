@@ -70,7 +70,7 @@ def parse_tile(b):
     L = layout()
     names = ["P", "LA", "LB", "nsegA", "nsegB", "pshift", "pad", "phys_size", "ngrid", "nblocked", "ntiles",
              "off_segA", "off_segB", "off_perm", "smem_bytes", "fast", "async_ok", "padA", "stage_elems",
-             "nstages", "off_gtab"]
+             "nstages", "off_gtab", "sigmaA"]
     t = {k: _i32(b, 4 * i) for i, k in enumerate(names)}
     t["divLA"] = _fd(b, L["off_divLA"])
     t["divLB"] = _fd(b, L["off_divLA"] + L["fastdiv_size"])
@@ -102,12 +102,14 @@ def check_staged_layout(t, vecA):
     inv[t["ptab"]] = np.arange(P, dtype=np.int64)
     p_of_q = inv[slot_q]
     assert (p_of_q >= 0).all()
-    stg = p_of_q + (p_of_q // t["LA"]) * t["padA"]
+    stg = p_of_q + (p_of_q // t["sigmaA"]) * t["padA"]
     assert np.array_equal(stg, t["gtab"]), "gtab disagrees with the staged layout"
     assert len(np.unique(t["gtab"])) == P and t["gtab"].max() < t["stage_elems"]
     assert t["stage_elems"] >= t["phys_size"]
     p = np.arange(0, P, vecA, dtype=np.int64)
-    assert ((p + (p // t["LA"]) * t["padA"]) % vecA == 0).all(), "staged vectors misaligned"
+    assert ((p + (p // t["sigmaA"]) * t["padA"]) % vecA == 0).all(), "staged vectors misaligned"
+    # a vector never straddles a padding point
+    assert t["sigmaA"] % vecA == 0
 
 
 def parse_row(b):

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include <new>
 #include <string>
 
@@ -52,17 +53,21 @@ static ttcb_status cuda_fail(cudaError_t e, const char* what) {
 
 static int variant_of(const ttcb_plan* p) { return p->beta_nonzero ? 2 : (p->streaming ? 1 : 0); }
 
-// Kernels whose dynamic shared memory may exceed the 48 KB default get the opt-in once.
+// Kernels whose shared memory (dynamic, plus the staged kernel's static copy of the descriptor
+// header) may exceed the 48 KB default get the opt-in once per device.
+static bool needs_large_smem(int dynamic_smem) { return dynamic_smem + (int)sizeof(TileDesc) > 48 * 1024; }
+
 static void allow_large_smem(const void* func) {
   static std::mutex mu;
-  static const void* done[512];
-  static int ndone = 0;
+  static std::vector<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(mu);
-  for (int i = 0; i < ndone; ++i)
-    if (done[i] == func) return;
+  for (const auto& x : done)
+    if (x.first == func && x.second == dev) return;
   cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaGetLastError();
-  if (ndone < 512) done[ndone++] = func;
+  done.emplace_back(func, dev);
 }
 
 static ttcb_status plan_finish_device(ttcb_plan* p) {
@@ -91,7 +96,7 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
   auto grid_for = [&](int kernel_id, int smem, int* out) -> ttcb_status {
     ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel_id, p->vecA, p->vecB, variant_of(p));
     if (!k.func) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-    if (smem > 48 * 1024) allow_large_smem(k.func);
+    if (needs_large_smem(smem)) allow_large_smem(k.func);
     int per_sm = 0;
     cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, smem);
     if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -116,8 +121,7 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (s != TTCB_OK) return s;
     }
     if (td->async_ok) {
-      s = grid_for(td->nstages == 3 ? TTCB_KERNEL_TILE_ASYNC3 : TTCB_KERNEL_TILE_ASYNC2, p->smem_async,
-                   &p->blocks_async);
+      s = grid_for(td->fast ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async, &p->blocks_async);
       if (s != TTCB_OK) return s;
     }
   }
@@ -206,7 +210,7 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
     const int want = p->tuning.tile_variant;
     const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
     if ((want == 0 || want == 3) && td->async_ok) {
-      kernel = td->nstages == 3 ? TTCB_KERNEL_TILE_ASYNC3 : TTCB_KERNEL_TILE_ASYNC2;
+      kernel = fast_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
       blocks = p->blocks_async;
       smem = p->smem_async;
     } else if ((want == 0 || want == 2) && fast_ok) {
@@ -217,7 +221,7 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
   }
   ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel, va, vb, variant_of(p));
   if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (smem > 48 * 1024) allow_large_smem(k.func);
+  if (needs_large_smem(smem)) allow_large_smem(k.func);
   e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), blocks);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return TTCB_OK;

@@ -57,8 +57,10 @@ struct TileDesc {
   int32_t stage_elems;// elements of one stage buffer (max of the staged layout and phys_size)
   int32_t nstages;    // pipeline depth (2 or 3)
   int32_t off_gtab;   // byte offset of gtab (uint16_t[P]) from the start of the descriptor
-  int32_t pad2_[3];
+  int32_t sigmaA;     // staged layout: element p at p + (p / sigmaA) * padA
+  int32_t pad2_[2];
   FastDiv divLA, divLB;
+  FastDiv divSigmaA;
   GridDimDesc g[TTCB_MAXR];
   BlockedDesc bd[2];
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
@@ -78,4 +80,6 @@ struct RowDesc {
 
 enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };
 // launch-time variant of a tile plan (never stored in a plan's kernel field)
-enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC2 = 4, TTCB_KERNEL_TILE_ASYNC3 = 5 };
+// Launch-time kernel choices for tile plans: register-prefetch kernel, staged kernel with offsets
+// computed from the run tables, staged kernel with offsets held in registers.
+enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5 };

@@ -44,7 +44,10 @@ __device__ __forceinline__ bool decode_tile(const TileDesc& d, uint32_t t, int64
     if (gd.blocked >= 0) {
       const int64_t left = gd.n - (int64_t)blk * gd.e;
       const int l = left < gd.e ? (int)left : gd.e;
-      lim[gd.blocked] = l;
+      if (gd.blocked == 0)  // constant indices keep lim[] in registers
+        lim[0] = l;
+      else
+        lim[1] = l;
       if (l < gd.e) full = false;
     }
   }
@@ -96,7 +99,7 @@ __device__ __forceinline__ void tile_ragged(const TileDesc& d, const TileTables&
         for (int b = 0; b < nb; ++b) {
           const uint32_t c = fdiv((uint32_t)p, d.bd[b].tsA);
           const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-          ok = ok && ((int)cc < lim[b]);
+          ok = ok && ((int)cc < (b == 0 ? lim[0] : lim[1]));
         }
         if (ok) {
           const int s = (int)fdiv((uint32_t)p, d.divLA);
@@ -122,7 +125,7 @@ __device__ __forceinline__ void tile_ragged(const TileDesc& d, const TileTables&
         for (int b = 0; b < nb; ++b) {
           const uint32_t c = fdiv((uint32_t)q, d.bd[b].tsB);
           const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-          ok = ok && ((int)cc < lim[b]);
+          ok = ok && ((int)cc < (b == 0 ? lim[0] : lim[1]));
         }
         if (ok) {
           const int s = (int)fdiv((uint32_t)q, d.divLB);
@@ -146,6 +149,16 @@ __device__ __forceinline__ void tile_ragged(const TileDesc& d, const TileTables&
     }
   }
   __syncthreads();
+}
+
+// The ragged path as a call, for kernels whose steady state keeps many offsets in registers: the
+// registers live across it are saved only when a ragged tile actually occurs.
+template <typename TA, typename TB, bool BETA, bool STREAM>
+__device__ __noinline__ void tile_ragged_call(const TileDesc& d, TileTables tt, int lim0, int lim1,
+                                              const TA* __restrict__ At, TB* __restrict__ Bt, TA alpha, TB beta,
+                                              TA* tile) {
+  const int lim[2] = {lim0, lim1};
+  tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, At, Bt, alpha, beta, tile);
 }
 
 // One tile with the generic table-driven loops: load phase (A runs -> alpha*A -> shared slots in B
@@ -405,9 +418,10 @@ __global__ void __launch_bounds__(kThreads, 3) tile_fast_kernel(const TileDesc* 
 // ------------------------------------------------------------------------------------------------
 // Staged tile kernel. A tiles are fetched with asynchronous global->shared copies (cp.async, no
 // register cost) into an S-stage ring, so S-1 tiles of loads stay in flight per CTA while the
-// current tile is written out. Shared memory holds A in A order (element p at p + (p/LA)*padA,
-// padA chosen by the planner against bank conflicts); the store phase gathers B order through
-// gtab[q] and applies alpha (and beta*B) on the way out.
+// current tile is written out. Shared memory holds A in A order (element p at
+// p + (p/sigmaA)*padA, the pair chosen by the planner against bank conflicts of the gather); the
+// store phase gathers B order through gtab[q] and applies alpha (and beta*B) on the way out. With
+// beta != 0 the B tile is staged the same way, in B order.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 template <int BYTES> __device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
@@ -423,11 +437,12 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Shared-memory layout of the staged kernel: [S stages][segA][segB][gtab].
-__host__ __device__ inline size_t stage_bytes(int stage_elems, int elem_bytes) {
-  return ((size_t)stage_elems * elem_bytes + 15) & ~size_t(15);
-}
+// Shared-memory layout of the staged kernel: S stages of [A tile (staged A order)][B tile (B order,
+// only when beta != 0)], then segA, segB, and gtab when the gather positions do not fit registers.
+constexpr int kRegPos = 16;  // gather positions per thread kept in registers (P <= kRegPos * kThreads)
+constexpr int kRegVec = 4;   // vectors per thread and side whose offsets the register path keeps
 
+// V consecutive 16-bit table entries (V-aligned) in one shared-memory access.
 template <typename T, int V> __device__ __forceinline__ void ld_u16s(const uint16_t* p, uint16_t* out) {
   if constexpr (V == 4) {
     const uint2 w = *reinterpret_cast<const uint2*>(p);
@@ -444,36 +459,101 @@ template <typename T, int V> __device__ __forceinline__ void ld_u16s(const uint1
   }
 }
 
-template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, int S>
-__global__ void __launch_bounds__(kThreads) tile_async_kernel(const TileDesc* __restrict__ desc,
-                                                              const TA* __restrict__ A, TB* __restrict__ B,
-                                                              TA alpha, TB beta) {
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline size_t async_stage_bytes(int stage_elems, int P, int ea, int eb, bool beta) {
+  return al16((size_t)stage_elems * ea) + (beta ? al16((size_t)P * eb) : 0);
+}
+__host__ __device__ inline size_t async_smem_bytes(int S, int stage_elems, int P, int nsegA, int nsegB, int ea, int eb,
+                                                   bool beta) {
+  return S * async_stage_bytes(stage_elems, P, ea, eb, beta) + 8 * (size_t)(nsegA + nsegB) +
+         (P > kRegPos * kThreads ? al16((size_t)2 * P) : 0);
+}
+
+// REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
+// vectors per thread and side whose offsets fit 32 bits): A source offsets rA, staged positions dA
+// (two per register), B offsets rB, gather positions gp (two per register; B vector
+// u = tid + u * kThreads, element j). Otherwise offsets are computed per vector from the run tables
+// in shared memory, with the gather positions in registers while P <= kRegPos * kThreads and in
+// shared memory beyond. The pipeline depth (2 or 3 stages) is the descriptor's.
+template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG>
+__global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc* __restrict__ desc,
+                                                                 const TA* __restrict__ A, TB* __restrict__ B,
+                                                                 TA alpha, TB beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TileDesc& d = *desc;
+  __shared__ TileDesc d;  // the descriptor header, read once per CTA
   const int tid = threadIdx.x;
+  for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
+    reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
+  __syncthreads();
   const int P = d.P, LA = d.LA, LB = d.LB, padA = d.padA;
-  const size_t sbytes = stage_bytes(d.stage_elems, sizeof(TA));
+  const int S = d.nstages;
+  const FastDiv divLA = d.divLA, divLB = d.divLB, divSig = d.divSigmaA;
+  const size_t a_bytes = al16((size_t)d.stage_elems * sizeof(TA));
+  const size_t sbytes = async_stage_bytes(d.stage_elems, P, sizeof(TA), sizeof(TB), BETA);
   int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + S * sbytes);
   int64_t* segB = segA + d.nsegA;
   uint16_t* gtab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+  const bool reg_pos = REG || P <= kRegPos * kThreads;
   const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
-  {
-    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
-    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
-    const uint32_t* gG = reinterpret_cast<const uint32_t*>(base + d.off_gtab);
-    uint32_t* sG = reinterpret_cast<uint32_t*>(gtab);
-    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
-    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
-    for (int i = tid; i < (P + 1) / 2; i += kThreads) sG[i] = gG[i];
-  }
+  const uint16_t* ggtab = reinterpret_cast<const uint16_t*>(base + d.off_gtab);
   const TileTables tg{reinterpret_cast<const int64_t*>(base + d.off_segA),
                       reinterpret_cast<const int64_t*>(base + d.off_segB),
                       reinterpret_cast<const uint16_t*>(base + d.off_perm)};
+  if (!REG) {
+    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = tg.segA[i];
+    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = tg.segB[i];
+    if (!reg_pos) {
+      const uint32_t* gG = reinterpret_cast<const uint32_t*>(ggtab);
+      uint32_t* sG = reinterpret_cast<uint32_t*>(gtab);
+      for (int i = tid; i < (P + 1) / 2; i += kThreads) sG[i] = gG[i];
+    }
+  }
+  const int nvA = P / VA, nvB = P / VB;
+  constexpr int kVecB = REG ? kRegVec : kRegPos / VB;  // B vectors per thread with positions in gp
+  constexpr int kGp = (kVecB * VB + 1) / 2;
+  uint32_t gp[kGp];
+  int32_t rA[REG ? kRegVec : 1], rB[REG ? kRegVec : 1];
+  uint32_t dA[REG ? kRegVec / 2 : 1];
+#pragma unroll
+  for (int e = 0; e < kGp; ++e) gp[e] = 0;
+  if (reg_pos) {
+#pragma unroll
+    for (int u = 0; u < kVecB; ++u) {
+      const int i = tid + u * kThreads;
+      if (i < nvB) {
+#pragma unroll
+        for (int j = 0; j < VB; ++j) {
+          const int e = u * VB + j;
+          const uint32_t v = ggtab[i * VB + j];
+          gp[e >> 1] |= (e & 1) ? (v << 16) : v;
+        }
+      }
+    }
+  }
+  if constexpr (REG) {
+#pragma unroll
+    for (int u = 0; u < kRegVec; ++u) {
+      const int i = tid + u * kThreads;
+      rA[u] = rB[u] = 0;
+      if (!(u & 1)) dA[u >> 1] = 0;
+      if (i < nvA) {
+        const int p = i * VA;
+        const int s = (int)fdiv((uint32_t)p, divLA);
+        const int sp = (int)fdiv((uint32_t)p, divSig);
+        rA[u] = (int32_t)(tg.segA[s] + (p - s * LA));
+        dA[u >> 1] |= (uint32_t)(p + sp * padA) << ((u & 1) * 16);
+      }
+      if (i < nvB) {
+        const int q = i * VB;
+        const int s = (int)fdiv((uint32_t)q, divLB);
+        rB[u] = (int32_t)(tg.segB[s] + (q - s * LB));
+      }
+    }
+  }
   __syncthreads();
 
   const uint32_t ntiles = (uint32_t)d.ntiles;
   const uint32_t G = gridDim.x;
-  const int nvA = P / VA, nvB = P / VB;
   const uint32_t stage0 = smem_u32(smem_raw);
 
   auto issue = [&](uint32_t t, int stage) {
@@ -482,68 +562,118 @@ __global__ void __launch_bounds__(kThreads) tile_async_kernel(const TileDesc* __
     int lim[2];
     if (!decode_tile(d, t, bA, bB, lim)) return;  // ragged tiles are read by the ragged path
     const TA* At = A + bA;
+    const TB* Bt = B + bB;
     const uint32_t sb = stage0 + (uint32_t)(stage * sbytes);
-    for (int i = tid; i < nvA; i += kThreads) {
-      const int p = i * VA;
-      const int s = (int)fdiv((uint32_t)p, d.divLA);
-      cp_async<VA * sizeof(TA)>(sb + (uint32_t)((p + s * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+    const uint32_t sbB = sb + (uint32_t)a_bytes;
+    if constexpr (REG) {
+#pragma unroll
+      for (int u = 0; u < kRegVec; ++u) {
+        const int i = tid + u * kThreads;
+        if (i < nvA)
+          cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu) * (uint32_t)sizeof(TA),
+                                    At + rA[u]);
+        if (BETA && i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
+      }
+    } else {
+      for (int i = tid; i < nvA; i += kThreads) {
+        const int p = i * VA;
+        const int s = (int)fdiv((uint32_t)p, divLA);
+        const int sp = (int)fdiv((uint32_t)p, divSig);
+        cp_async<VA * sizeof(TA)>(sb + (uint32_t)((p + sp * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+      }
+      if (BETA) {
+        for (int i = tid; i < nvB; i += kThreads) {
+          const int q = i * VB;
+          const int s = (int)fdiv((uint32_t)q, divLB);
+          cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(q * sizeof(TB)), Bt + (segB[s] + (q - s * LB)));
+        }
+      }
     }
   };
 
+  auto out_vec = [&](const TA* st, const TB* sB, int q, const uint16_t* pos, TB* dst) {
+    Vec<TB, VB> out;
+    Vec<TB, VB> bv;
+    if (BETA) bv = *reinterpret_cast<const Vec<TB, VB>*>(sB + q);
 #pragma unroll
+    for (int j = 0; j < VB; ++j) {
+      const TA tj = scale_a(alpha, st[pos[j]]);
+      if (BETA)
+        out.v[j] = combine<TA, TB>(tj, bv.v[j], beta);
+      else
+        out.v[j] = finish<TA, TB>(tj);
+    }
+    st_vec<TB, VB>(dst, out, STREAM);
+  };
+  auto reg_pos_of = [&](int u, uint16_t* pos) {
+#pragma unroll
+    for (int j = 0; j < VB; ++j) {
+      const int e = u * VB + j;
+      pos[j] = (uint16_t)((e & 1) ? (gp[e >> 1] >> 16) : (gp[e >> 1] & 0xffffu));
+    }
+  };
+
   for (int k = 0; k < S - 1; ++k) {
     issue(blockIdx.x + k * G, k);
     cp_async_commit();
   }
+  int cur = 0;  // ring slot of tile k; the slot S - 1 ahead is the one before it
   for (uint32_t k = 0;; ++k) {
     const uint32_t t = blockIdx.x + k * G;
     if (t >= ntiles) break;
-    issue(t + (S - 1) * G, (int)((k + S - 1) % S));
+    issue(t + (S - 1) * G, cur == 0 ? S - 1 : cur - 1);
     cp_async_commit();
     int64_t bA, bB;
     int lim[2];
     const bool full = decode_tile(d, t, bA, bB, lim);
     TB* Bt = B + bB;
-    TA* st = reinterpret_cast<TA*>(smem_raw + (k % S) * sbytes);
-    cp_async_wait<S - 1>();
+    unsigned char* stage = smem_raw + cur * sbytes;
+    TA* st = reinterpret_cast<TA*>(stage);
+    const TB* sB = reinterpret_cast<const TB*>(stage + a_bytes);
+    if (S == 3)
+      cp_async_wait<2>();
+    else
+      cp_async_wait<1>();
     __syncthreads();
     if (full) {
-      for (int i0 = tid; i0 < nvB; i0 += kThreads * kUnroll) {
-        int64_t o[kUnroll];
-        Vec<TB, VB> bv[kUnroll];
+      if constexpr (REG) {
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          const int i = i0 + u * kThreads;
-          if (i < nvB) {
-            const int q = i * VB;
-            const int s = (int)fdiv((uint32_t)q, d.divLB);
-            o[u] = segB[s] + (q - s * LB);
-            if (BETA) bv[u] = ld_stream<TB, VB>(Bt + o[u]);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-          const int i = i0 + u * kThreads;
+        for (int u = 0; u < kRegVec; ++u) {
+          const int i = tid + u * kThreads;
           if (i < nvB) {
             uint16_t pos[VB];
-            ld_u16s<TA, VB>(gtab + i * VB, pos);
-            Vec<TB, VB> out;
+            reg_pos_of(u, pos);
+            out_vec(st, sB, i * VB, pos, Bt + rB[u]);
+          }
+        }
+      } else {
+        if (reg_pos) {
 #pragma unroll
-            for (int j = 0; j < VB; ++j) {
-              const TA tj = scale_a(alpha, st[pos[j]]);
-              if (BETA)
-                out.v[j] = combine<TA, TB>(tj, bv[u].v[j], beta);
-              else
-                out.v[j] = finish<TA, TB>(tj);
+          for (int u = 0; u < kVecB; ++u) {
+            const int i = tid + u * kThreads;
+            if (i < nvB) {
+              const int q = i * VB;
+              const int s = (int)fdiv((uint32_t)q, divLB);
+              uint16_t pos[VB];
+              reg_pos_of(u, pos);
+              out_vec(st, sB, q, pos, Bt + (segB[s] + (q - s * LB)));
             }
-            st_vec<TB, VB>(Bt + o[u], out, STREAM);
+          }
+        } else {
+          for (int i = tid; i < nvB; i += kThreads) {
+            const int q = i * VB;
+            const int s = (int)fdiv((uint32_t)q, divLB);
+            uint16_t pos[VB];
+            ld_u16s<TA, VB>(gtab + q, pos);
+            out_vec(st, sB, q, pos, Bt + (segB[s] + (q - s * LB)));
           }
         }
       }
     } else {
-      tile_ragged<TA, TB, BETA, STREAM>(d, tg, lim, A + bA, Bt, alpha, beta, st);
+      tile_ragged_call<TA, TB, BETA, STREAM>(d, tg, lim[0], lim[1], A + bA, Bt, alpha, beta, st);
     }
     __syncthreads();
+    cur = cur + 1 == S ? 0 : cur + 1;
   }
   cp_async_wait<0>();
 }

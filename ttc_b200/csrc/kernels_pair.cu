@@ -53,7 +53,7 @@ using TB = float2;
 #define PAIR_BATCH_FN pick_batch_zc
 #endif
 
-template <int VA, int VB, bool BETA, bool STREAM, int S>
+template <int VA, int VB, bool BETA, bool STREAM, bool REG>
 static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
                                 cudaStream_t stream, int blocks) {
   TA al;
@@ -61,41 +61,41 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
-  tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, S><<<blocks, kThreads, p->smem_async, stream>>>(
+  tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG><<<blocks, kThreads, p->smem_async, stream>>>(
       reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
   return cudaGetLastError();
 }
 
-template <int VA, int VB, int S>
+template <int VA, int VB, bool REG>
 static KernelRef async_ref(int variant) {
   KernelRef r;
   if (variant == 2) {
-    r.fn = &launch_async<VA, VB, true, false, S>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, S>);
+    r.fn = &launch_async<VA, VB, true, false, REG>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, REG>);
   } else if (variant == 1) {
-    r.fn = &launch_async<VA, VB, false, true, S>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, S>);
+    r.fn = &launch_async<VA, VB, false, true, REG>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, REG>);
   } else {
-    r.fn = &launch_async<VA, VB, false, false, S>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, S>);
+    r.fn = &launch_async<VA, VB, false, false, REG>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, REG>);
   }
   return r;
 }
 
-template <int VA, int S>
+template <int VA, bool REG>
 static KernelRef async_ref_b(int vb, int variant) {
   constexpr int MB = 16 / sizeof(TB);
-  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), S>(variant);
-  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), S>(variant);
-  return async_ref<VA, 1, S>(variant);
+  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), REG>(variant);
+  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), REG>(variant);
+  return async_ref<VA, 1, REG>(variant);
 }
 
-template <int S>
+template <bool REG>
 static KernelRef async_ref_ab(int va, int vb, int variant) {
   constexpr int MA = 16 / sizeof(TA);
-  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), S>(vb, variant);
-  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), S>(vb, variant);
-  return async_ref_b<1, S>(vb, variant);
+  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), REG>(vb, variant);
+  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), REG>(vb, variant);
+  return async_ref_b<1, REG>(vb, variant);
 }
 
 template <int VA, int VB, bool BETA, bool STREAM, bool FAST>
@@ -191,8 +191,8 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
     return row_ref<1>(variant);
   }
   if (kernel == TTCB_KERNEL_TILE_FAST) return tile_ref_ab<true>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC2) return async_ref_ab<2>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC3) return async_ref_ab<3>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true>(va, vb, variant);
   return tile_ref_ab<false>(va, vb, variant);
 }
 

@@ -106,11 +106,12 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   int va = p.vecA, vb = p.vecB;
   while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
   while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
-  const int kernel = td->nstages == 3 ? TTCB_KERNEL_TILE_ASYNC3 : TTCB_KERNEL_TILE_ASYNC2;
+  const bool reg = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
+  const int kernel = reg ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
   const int variant = p.beta_nonzero ? 2 : (p.streaming ? 1 : 0);
   ttcb::KernelRef k = ttcb::pick_kernel(p.ta, p.tb, kernel, va, vb, variant);
   if (!k.fn) return na_fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (p.smem_async > 48 * 1024) {
+  if (p.smem_async + (int)sizeof(TileDesc) > 48 * 1024) {
     e = cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_async);
     if (e != cudaSuccess) return na_cuda(e, "cudaFuncSetAttribute");
   }

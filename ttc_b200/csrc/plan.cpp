@@ -11,6 +11,7 @@
 // The blocking/loop-order search of GPUtransposeGenerator.py:165-285 is replaced by a cost model
 // over multi-dimensional tiles (below) whose knobs the autotuner searches.
 #include "plan.h"
+#include "kernels.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -373,44 +374,65 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     p_of_q[q] = pp;
     if (pp % c.LA == 0) segA[pp / c.LA] = offA;
   }
-  // Staged layout of the asynchronous-copy kernel: element p at p + (p / LA) * padA. The pad is the
-  // multiple of the A vector that minimises shared-memory bank conflicts of the store-phase gather,
-  // replayed on the host for the first warps (32 lanes, 4-byte banks).
+  // Staged layout of the asynchronous-copy kernel: element p at p + (p / sigma) * padA. sigma (a
+  // multiple of the A vector that divides into whole vectors) and padA (a multiple of the A vector)
+  // are the pair that minimises shared-memory bank conflicts of the store-phase gather, replayed on
+  // the host for the first warps (32 lanes, 4-byte banks).
   const int EAw = EA >= 4 ? EA / 4 : 1;
-  auto staged = [&](int64_t pp, int64_t padA) { return pp + (pp / c.LA) * padA; };
+  int64_t sigma = c.LA;
+  auto staged = [&](int64_t pp, int64_t padA) { return pp + (pp / sigma) * padA; };
+  // A warp's 8-byte loads are served per half-warp and its 16-byte loads per quarter-warp, so the
+  // wavefronts of one load are the sum over those lane groups of the busiest bank's count.
+  const int group = 32 / EAw;
   auto gather_cost = [&](int64_t padA) {
     int64_t cost = 0;
     const int vb = c.vecB;
     for (int w = 0; w < 4; ++w) {
       for (int j = 0; j < vb; ++j) {
-        int cnt[32] = {0};
-        int mx = 0;
-        for (int lane = 0; lane < 32; ++lane) {
-          int64_t i = (int64_t)w * 32 + lane;
-          if (i * vb >= P) continue;
-          int64_t word = staged(p_of_q[i * vb + j], padA) * EAw;
-          for (int x = 0; x < EAw; ++x) {
-            int b = (int)((word + x) & 31);
-            mx = std::max(mx, ++cnt[b]);
+        for (int g0 = 0; g0 < 32; g0 += group) {
+          int cnt[32] = {0};
+          int mx = 0;
+          for (int lane = g0; lane < g0 + group; ++lane) {
+            int64_t i = (int64_t)w * 32 + lane;
+            if (i * vb >= P) continue;
+            int64_t word = staged(p_of_q[i * vb + j], padA) * EAw;
+            for (int x = 0; x < EAw; ++x) {
+              int b = (int)((word + x) & 31);
+              mx = std::max(mx, ++cnt[b]);
+            }
           }
+          cost += mx;
         }
-        cost += mx;
       }
     }
     return cost;
   };
   int64_t padA = 0;
   {
-    int64_t best = gather_cost(0);
-    for (int k = 1; k <= 8; ++k) {
-      int64_t cand = (int64_t)k * c.vecA;
-      if (cand > 32) break;
-      int64_t cc = gather_cost(cand);
-      if (cc < best) {
-        best = cc;
-        padA = cand;
+    // periods: the A run, small multiples of the A-order stride of each tile dimension, and every
+    // multiple of the A vector up to 64 elements
+    std::vector<int64_t> sigmas = {c.LA};
+    for (int d : aord)
+      for (int64_t m = 1; m <= 8; m *= 2)
+        if (tsA[d] > 1 && m * tsA[d] < P && (m * tsA[d]) % c.vecA == 0) sigmas.push_back(m * tsA[d]);
+    for (int64_t k = c.vecA; k <= 64 && k < P; k += c.vecA) sigmas.push_back(k);
+    int64_t best_cost = -1, best_sigma = c.LA, best_pad = 0;
+    for (int64_t sg : sigmas) {
+      sigma = sg;
+      for (int k = 0; k <= 8; ++k) {
+        const int64_t cand = (int64_t)k * c.vecA;
+        if (k && (cand > 32 || cand > sg)) break;
+        if ((P - 1) / sg * cand + P > 65535) continue;
+        const int64_t cc = gather_cost(cand);
+        if (best_cost < 0 || cc < best_cost) {
+          best_cost = cc;
+          best_sigma = sg;
+          best_pad = cand;
+        }
       }
     }
+    sigma = best_sigma;
+    padA = best_pad;
   }
   const int64_t staged_size = staged(P - 1, padA) + 1;
   std::vector<uint16_t> gtab(P);
@@ -492,12 +514,19 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     for (int64_t x : segB) mB = std::max(mB, x + c.LB);
     td.fast = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && P / c.vecA <= 1024 && P / c.vecB <= 1024) ? 1 : 0;
     td.padA = (int32_t)padA;
+    td.sigmaA = (int32_t)sigma;
+    td.divSigmaA = make_fastdiv((uint32_t)sigma);
     td.stage_elems = (int32_t)std::max<int64_t>(staged_size, phys_size);
-    const int64_t sb = al16(td.stage_elems * EA);
-    const int64_t tables = 8 * nsegA + 8 * nsegB + al16(2 * P);
-    td.nstages = (3 * sb + tables <= 80 * 1024) ? 3 : 2;
-    td.async_ok = (mA < (int64_t(1) << 31) && td.stage_elems < 65536 && td.nstages * sb + tables <= 200 * 1024) ? 1 : 0;
-    p->smem_async = (int)(td.nstages * sb + tables);
+    const bool beta = p->beta_nonzero != 0;
+    const int EB = dtype_bytes(p->tb);
+    auto smem_for = [&](int S) {
+      return (int64_t)ttcb::async_smem_bytes(S, td.stage_elems, (int)P, (int)nsegA, (int)nsegB, EA, EB, beta);
+    };
+    // three stages while four CTAs still fit an SM (about 56 KB each), else two
+    td.nstages = smem_for(3) <= 56 * 1024 ? 3 : 2;
+    td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
+                   smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
+    p->smem_async = (int)smem_for(td.nstages);
   }
 
   p->host_desc.assign(off, 0);
@@ -717,7 +746,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
     o << ",\"tile\":{\"P\":" << t->P << ",\"LA\":" << t->LA << ",\"LB\":" << t->LB << ",\"ntiles\":" << t->ntiles
       << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
-      << ",\"padA\":" << t->padA << ",\"stages\":" << t->nstages << "}";
+      << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages << "}";
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     o << ",\"row\":{\"w\":" << rd->w << ",\"chunk\":" << rd->chunk << ",\"units\":" << rd->nunits << "}";
