@@ -49,6 +49,12 @@ def parse():
     ap.add_argument("--cpu-sample-cases", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched"],
+                    help="sweep: the 64-case 200 MiB sweep (default); batched: 4096 small transpositions "
+                         "in one persistent launch against per-call launches")
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--batch-tuning", default="search", choices=["search", "default"],
+                    help="per-problem schedules: measured search (the autotuner) or the planner default")
     return ap.parse_args()
 
 
@@ -106,6 +112,13 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def device_uuid(dev):
+    """nvidia-smi's id of a torch device (its UUID), so the sampler reads this GPU only."""
+    import torch
+    uuid = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
+    return f"GPU-{uuid}" if uuid is not None else None
 
 
 def measured_peak_gbs():
@@ -212,6 +225,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.workload == "batched":
+        return run_batched(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
@@ -253,10 +268,7 @@ def main():
         step()
     torch.cuda.synchronize()
 
-    props = torch.cuda.get_device_properties(dev)
-    uuid = getattr(props, "uuid", None)
-    dev_id = f"GPU-{uuid}" if uuid is not None else None
-    sampler = ClockSampler(dev_id).start()
+    sampler = ClockSampler(device_uuid(dev)).start()
     time.sleep(0.3)
     evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in items]
            for _ in range(args.steps)]
@@ -336,6 +348,10 @@ def main():
 
 
 def run_e2e(args, items, stream, dev, world):
+    """The metric through the public call from pinned host buffers: per case, A (and B when
+    beta != 0) is copied in, transposed and B copied out. Copies in and out run on their own
+    streams so that PCIe carries both directions at once (case i+1 comes in while case i goes out);
+    each case's copy-in, kernel and copy-out are ordered by events."""
     import torch
     sub = items[: max(1, min(args.e2e_cases, len(items)))]
     host = []
@@ -349,14 +365,21 @@ def run_e2e(args, items, stream, dev, world):
               for (c, _, _, _), (hA, hB) in zip(sub, host))
     d2h = sum(hB.numel() * hB.element_size() for _, hB in host)
     outs = [torch.empty_like(hB, pin_memory=True) for _, hB in host]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
 
     def one():
         for (c, plan, A, B), (hA, hB), o in zip(sub, host, outs):
-            A.copy_(hA, non_blocking=True)
-            if c["beta"] != 0:
-                B.copy_(hB, non_blocking=True)
+            with torch.cuda.stream(s_in):
+                s_in.wait_stream(s_out)  # the previous step's copy-out of this B is done
+                A.copy_(hA, non_blocking=True)
+                if c["beta"] != 0:
+                    B.copy_(hB, non_blocking=True)
+            stream.wait_stream(s_in)
             plan(A, B, c["alpha"], c["beta"], stream)
-            o.copy_(B, non_blocking=True)
+            s_out.wait_stream(stream)
+            with torch.cuda.stream(s_out):
+                o.copy_(B, non_blocking=True)
+        stream.wait_stream(s_out)
 
     one()
     torch.cuda.synchronize()
@@ -366,6 +389,8 @@ def run_e2e(args, items, stream, dev, world):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
+    s_in.wait_stream(stream)
+    s_out.wait_stream(stream)
     for _ in range(args.e2e_steps):
         one()
     t1.record(stream)
@@ -379,7 +404,144 @@ def run_e2e(args, items, stream, dev, world):
     nbytes = sum(p.bytes for _, p, _, _ in sub)
     return {"value": round(nbytes * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "cases": len(sub), "ms_per_step": round(ms, 3),
-            "note": "pinned host A/B copied in, result copied out, per case, inside the timed region"}
+            "note": ("pinned host A (and B when beta != 0) copied in and B copied out for every case inside the "
+                     "timed region; copy-in and copy-out on separate streams (PCIe both directions)")}
+
+
+# ------------------------------------------------------------------------------------------------
+BATCH_WORKLOAD = ("batched4096: seeded rank-3..5 fp32 transpositions, random perms, element counts "
+                  "log-normal median 64Ki clipped to [1Ki, 1Mi], alpha=1 beta=0")
+
+
+def run_batched(args, rank, world, local):
+    """Batched mode: every problem of the batch in one persistent launch (plain and replayed from a
+    captured CUDA graph) against the same problems launched one call at a time: a Python loop over
+    the public call, that loop captured into a CUDA graph, and a loop that synchronizes after every
+    call as TTC's generated wrapper does. Every batched result is compared bit for bit with the
+    per-call result."""
+    import torch
+    import torch.distributed as dist
+    import ttc_b200.workloads as wl
+    from ttc_b200 import Plan
+    from ttc_b200.autotune import Bench, Problem, tune_for_batch
+    from ttc_b200.batched import Batch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    cases = wl.batched_cases(seed=7 + 1000 * rank, count=args.batch_count)
+    t_tune = time.perf_counter()
+    plans, As, Bs, Cs = [], [], [], []
+    gen = torch.Generator(device=dev)
+    for k, c in enumerate(cases):
+        n = math.prod(c["size"])
+        tu = None
+        if args.batch_tuning == "search":
+            tu = tune_for_batch(Problem(c["perm"], c["size"], "s"), max_impl=6, reps=2) or None
+        plans.append(Plan(c["perm"], c["size"], "s", False, tuning=tu))
+        gen.manual_seed(1_000_000 + k)
+        As.append(torch.rand(n, device=dev, generator=gen).mul_(2).sub_(1))
+        Bs.append(torch.full((n,), float("nan"), device=dev))
+        Cs.append(torch.full((n,), float("nan"), device=dev))
+    t_tune = time.perf_counter() - t_tune
+    batch = Batch(plans, As, Bs, alpha=1.0)
+    total = batch.bytes
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    def per_call():
+        for p, a, cbuf in zip(plans, As, Cs):
+            p(a, cbuf, 1.0, 0.0, stream)
+
+    def per_call_sync():
+        for p, a, cbuf in zip(plans, As, Cs):
+            p(a, cbuf, 1.0, 0.0, stream)
+            torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        batch.launch(stream)
+        batch.launch(stream, graph=True)
+        per_call()
+    batch.check_status(stream)
+    g = torch.cuda.CUDAGraph()
+    s2 = torch.cuda.Stream()
+    s2.wait_stream(stream)
+    with torch.cuda.stream(s2):
+        with torch.cuda.graph(g, stream=s2):
+            for p, a, cbuf in zip(plans, As, Cs):
+                p(a, cbuf, 1.0, 0.0, s2)
+    stream.wait_stream(s2)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(device_uuid(dev)).start()
+    time.sleep(0.3)
+    ms_graph = timed(lambda: batch.launch(stream, graph=True), args.steps)
+    clocks = sampler.stop()
+    ms_plain = timed(lambda: batch.launch(stream), args.steps)
+    ms_calls = timed(per_call, max(1, args.steps // 2))
+    ms_calls_graph = timed(g.replay, args.steps)
+    ms_calls_sync = timed(per_call_sync, 1)
+    batch.check_status(stream)
+
+    # every batched result against the per-call result, bit for bit
+    per_call()
+    torch.cuda.synchronize()
+    mismatches = sum(0 if torch.equal(b.view(torch.int32), cbuf.view(torch.int32)) else 1 for b, cbuf in zip(Bs, Cs))
+    gbs = lambda ms: round(total * world / (ms / 1e3) / 1e9, 2)
+    kinds = {}
+    for p in plans:
+        k = p.describe()["kernel"]
+        kinds[k] = kinds.get(k, 0) + 1
+    if rank == 0:
+        line = {"metric": "batched transpose GB/s (one persistent launch under a CUDA graph)",
+                "value": gbs(ms_graph), "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_graph, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded uniform[-1,1])",
+                "config": {"workload": BATCH_WORKLOAD, "problems": len(cases), "bytes_per_step_per_gpu": total,
+                           "schedules": ("measured search per problem over tile shape x raster order "
+                                         "(table-driven kernel, 6 candidates, 2 reps)"
+                                         if args.batch_tuning == "search" else "planner default"),
+                           "tuning_seconds": round(t_tune, 1), "plan_kinds": kinds,
+                           "l2": f"{total / 1e9:.2f} GB per step, larger than L2"},
+                "batched_plain_launch": {"GBps": gbs(ms_plain), "ms": round(ms_plain, 4)},
+                "per_call": {"python_loop": {"GBps": gbs(ms_calls), "ms": round(ms_calls, 3)},
+                             "graph_of_calls": {"GBps": gbs(ms_calls_graph), "ms": round(ms_calls_graph, 3)},
+                             "sync_each_call": {"GBps": gbs(ms_calls_sync), "ms": round(ms_calls_sync, 3)}},
+                "speedup": {"vs_python_loop": round(ms_calls / ms_graph, 2),
+                            "vs_graph_of_calls": round(ms_calls_graph / ms_graph, 2),
+                            "vs_sync_each_call": round(ms_calls_sync / ms_graph, 2)},
+                "check": {"problems": len(cases), "mismatches_vs_per_call": mismatches},
+                "clocks": clocks, "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+    del g
+    batch.close()
+    for p in plans:
+        p.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 1 if mismatches else 0
 
 
 if __name__ == "__main__":

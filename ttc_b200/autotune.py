@@ -202,3 +202,22 @@ def search(p: Problem, max_impl: int = 200, reps: int = 5, verify: bool = True, 
         raise RuntimeError(f"[TTC] ERROR: {len(bad)} schedules disagree with the first one: {bad[0].tuning}")
     best = min(res, key=lambda r: r.time_ms)
     return {"best": best, "results": res, "seconds": time.perf_counter() - t0, "candidates": len(cands)}
+
+
+def batch_space(dtype: str) -> dict:
+    """The knobs that matter inside the batched kernel: tile shape and raster order (it runs every
+    tile with the table-driven body on its own persistent grid, so the kernel variant and CTA count
+    of a plain launch do not apply)."""
+    s = knob_space(dtype)
+    return {"tile_elems": s["tile_elems"], "run_bytes": s["run_bytes"], "tile_variant": [1],
+            "loop_order": [0, 1], "blocks": [0]}
+
+
+def tune_for_batch(p: Problem, max_impl: int = 6, reps: int = 2, bench: Optional[Bench] = None) -> dict:
+    """Measured search of one batched problem's schedule (timed with the table-driven kernel the
+    batch runs). Returns the fastest tuning."""
+    cands = candidate_tunings(p, max_impl, batch_space(p.dtype))
+    if len(cands) <= 1:
+        return cands[0] if cands else {}
+    res = measure(p, cands, reps=reps, verify=False, bench=bench)
+    return min(res, key=lambda r: r.time_ms).tuning

@@ -121,7 +121,8 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (s != TTCB_OK) return s;
     }
     if (td->async_ok) {
-      s = grid_for(td->fast ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async, &p->blocks_async);
+      s = grid_for(td->reg_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async,
+                   &p->blocks_async);
       if (s != TTCB_OK) return s;
     }
   }
@@ -210,7 +211,7 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
     const int want = p->tuning.tile_variant;
     const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
     if ((want == 0 || want == 3) && td->async_ok) {
-      kernel = fast_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
+      kernel = (fast_ok && td->reg_ok) ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
       blocks = p->blocks_async;
       smem = p->smem_async;
     } else if ((want == 0 || want == 2) && fast_ok) {

@@ -58,7 +58,8 @@ struct TileDesc {
   int32_t nstages;    // pipeline depth (2 or 3)
   int32_t off_gtab;   // byte offset of gtab (uint16_t[P]) from the start of the descriptor
   int32_t sigmaA;     // staged layout: element p at p + (p / sigmaA) * padA
-  int32_t pad2_[2];
+  int32_t reg_ok;     // 1: fast, and the staged tile's byte offsets fit 16 bits (register path)
+  int32_t pad2_[1];
   FastDiv divLA, divLB;
   FastDiv divSigmaA;
   GridDimDesc g[TTCB_MAXR];

@@ -34,6 +34,7 @@ __device__ __forceinline__ bool decode_tile(const TileDesc& d, uint32_t t, int64
   bool full = true;
   lim[0] = lim[1] = 0x7fffffff;
   const int ng = d.ngrid;
+#pragma unroll 1  // a rolled loop keeps the callers' register budget
   for (int g = 0; g < ng; ++g) {
     const GridDimDesc& gd = d.g[g];
     const uint32_t q = fdiv(t, gd.div);
@@ -440,6 +441,12 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // Shared-memory layout of the staged kernel: S stages of [A tile (staged A order)][B tile (B order,
 // only when beta != 0)], then segA, segB, and gtab when the gather positions do not fit registers.
 constexpr int kRegPos = 16;  // gather positions per thread kept in registers (P <= kRegPos * kThreads)
+// Resident CTAs per SM that the staged kernel's register budget is sized for: with beta != 0 and
+// wide accesses, 3 (80 registers: the extra B stream keeps more offsets live); otherwise 4 (64
+// registers: narrow accesses need the extra warps to cover their larger instruction count).
+constexpr int async_min_blocks(int bytes_a, int bytes_b, bool beta) {
+  return (beta && bytes_a + bytes_b >= 24) ? 3 : 4;
+}
 constexpr int kRegVec = 4;   // vectors per thread and side whose offsets the register path keeps
 
 // V consecutive 16-bit table entries (V-aligned) in one shared-memory access.
@@ -469,48 +476,60 @@ __host__ __device__ inline size_t async_smem_bytes(int S, int stage_elems, int P
          (P > kRegPos * kThreads ? al16((size_t)2 * P) : 0);
 }
 
+// Decoded tile, shared by the CTA: thread 0 decodes each tile once, S iterations ahead, into a
+// four-entry ring (tile j of this CTA in entry j & 3). The entry written in iteration k is read
+// only after that iteration's barriers, and its previous tile was consumed before them.
+struct TileInfo {
+  int64_t bA, bB;
+  int32_t state;  // 1: complete tile, 0: ragged tile, -1: past the last tile
+  int32_t lim0, lim1, pad_;
+};
+
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
-// vectors per thread and side whose offsets fit 32 bits): A source offsets rA, staged positions dA
-// (two per register), B offsets rB, gather positions gp (two per register; B vector
-// u = tid + u * kThreads, element j). Otherwise offsets are computed per vector from the run tables
-// in shared memory, with the gather positions in registers while P <= kRegPos * kThreads and in
-// shared memory beyond. The pipeline depth (2 or 3 stages) is the descriptor's.
+// vectors per thread and side whose offsets fit 32 bits and whose staged bytes fit 16 bits): A
+// source offsets rA, staged byte offsets dA (two per register), B offsets rB, gather byte offsets
+// gp (two per register; B vector u = tid + u * kThreads, element j). Otherwise offsets are computed
+// per vector from the run tables in shared memory, with the gather positions in registers while
+// P <= kRegPos * kThreads and in shared memory beyond. The pipeline depth (2 or 3 stages) is the
+// descriptor's.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG>
-__global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc* __restrict__ desc,
-                                                                 const TA* __restrict__ A, TB* __restrict__ B,
-                                                                 TA alpha, TB beta) {
+__global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
+    tile_async_kernel(
+    const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
+  __shared__ TileInfo info[4];
   const int tid = threadIdx.x;
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
     reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
   __syncthreads();
-  const int P = d.P, LA = d.LA, LB = d.LB, padA = d.padA;
+  const int P = d.P;
   const int S = d.nstages;
-  const FastDiv divLA = d.divLA, divLB = d.divLB, divSig = d.divSigmaA;
-  const size_t a_bytes = al16((size_t)d.stage_elems * sizeof(TA));
-  const size_t sbytes = async_stage_bytes(d.stage_elems, P, sizeof(TA), sizeof(TB), BETA);
+  const uint32_t a_bytes = (uint32_t)al16((size_t)d.stage_elems * sizeof(TA));
+  const uint32_t sbytes = (uint32_t)async_stage_bytes(d.stage_elems, P, sizeof(TA), sizeof(TB), BETA);
   int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + S * sbytes);
   int64_t* segB = segA + d.nsegA;
   uint16_t* gtab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
   const bool reg_pos = REG || P <= kRegPos * kThreads;
   const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
   const uint16_t* ggtab = reinterpret_cast<const uint16_t*>(base + d.off_gtab);
-  const TileTables tg{reinterpret_cast<const int64_t*>(base + d.off_segA),
-                      reinterpret_cast<const int64_t*>(base + d.off_segB),
-                      reinterpret_cast<const uint16_t*>(base + d.off_perm)};
-  if (!REG) {
-    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = tg.segA[i];
-    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = tg.segB[i];
-    if (!reg_pos) {
-      const uint32_t* gG = reinterpret_cast<const uint32_t*>(ggtab);
-      uint32_t* sG = reinterpret_cast<uint32_t*>(gtab);
-      for (int i = tid; i < (P + 1) / 2; i += kThreads) sG[i] = gG[i];
+  {
+    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
+    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
+    if (!REG) {
+      for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+      for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
+      if (!reg_pos) {
+        const uint32_t* gG = reinterpret_cast<const uint32_t*>(ggtab);
+        uint32_t* sG = reinterpret_cast<uint32_t*>(gtab);
+        for (int i = tid; i < (P + 1) / 2; i += kThreads) sG[i] = gG[i];
+      }
     }
   }
   const int nvA = P / VA, nvB = P / VB;
   constexpr int kVecB = REG ? kRegVec : kRegPos / VB;  // B vectors per thread with positions in gp
   constexpr int kGp = (kVecB * VB + 1) / 2;
+  // gather positions: byte offsets in the register path, element positions otherwise
   uint32_t gp[kGp];
   int32_t rA[REG ? kRegVec : 1], rB[REG ? kRegVec : 1];
   uint32_t dA[REG ? kRegVec / 2 : 1];
@@ -524,13 +543,17 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
 #pragma unroll
         for (int j = 0; j < VB; ++j) {
           const int e = u * VB + j;
-          const uint32_t v = ggtab[i * VB + j];
+          const uint32_t v = (uint32_t)ggtab[i * VB + j] * (REG ? (uint32_t)sizeof(TA) : 1u);
           gp[e >> 1] |= (e & 1) ? (v << 16) : v;
         }
       }
     }
   }
   if constexpr (REG) {
+    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
+    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
+    const int LA = d.LA, LB = d.LB, padA = d.padA;
+    const FastDiv divLA = d.divLA, divLB = d.divLB, divSig = d.divSigmaA;
 #pragma unroll
     for (int u = 0; u < kRegVec; ++u) {
       const int i = tid + u * kThreads;
@@ -540,41 +563,51 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
         const int p = i * VA;
         const int s = (int)fdiv((uint32_t)p, divLA);
         const int sp = (int)fdiv((uint32_t)p, divSig);
-        rA[u] = (int32_t)(tg.segA[s] + (p - s * LA));
-        dA[u >> 1] |= (uint32_t)(p + sp * padA) << ((u & 1) * 16);
+        rA[u] = (int32_t)(gA[s] + (p - s * LA));
+        dA[u >> 1] |= ((uint32_t)(p + sp * padA) * (uint32_t)sizeof(TA)) << ((u & 1) * 16);
       }
       if (i < nvB) {
         const int q = i * VB;
         const int s = (int)fdiv((uint32_t)q, divLB);
-        rB[u] = (int32_t)(tg.segB[s] + (q - s * LB));
+        rB[u] = (int32_t)(gB[s] + (q - s * LB));
       }
     }
   }
-  __syncthreads();
 
   const uint32_t ntiles = (uint32_t)d.ntiles;
   const uint32_t G = gridDim.x;
   const uint32_t stage0 = smem_u32(smem_raw);
 
-  auto issue = [&](uint32_t t, int stage) {
-    if (t >= ntiles) return;
+  auto decode_into = [&](uint32_t t, TileInfo& ti) {
+    if (t >= ntiles) {
+      ti.state = -1;
+      return;
+    }
     int64_t bA, bB;
     int lim[2];
-    if (!decode_tile(d, t, bA, bB, lim)) return;  // ragged tiles are read by the ragged path
-    const TA* At = A + bA;
-    const TB* Bt = B + bB;
-    const uint32_t sb = stage0 + (uint32_t)(stage * sbytes);
-    const uint32_t sbB = sb + (uint32_t)a_bytes;
+    ti.state = decode_tile(d, t, bA, bB, lim) ? 1 : 0;
+    ti.bA = bA;
+    ti.bB = bB;
+    ti.lim0 = lim[0];
+    ti.lim1 = lim[1];
+  };
+
+  auto issue = [&](const TileInfo& ti, int stage) {
+    if (ti.state != 1) return;  // ragged tiles are read by the ragged path
+    const TA* At = A + ti.bA;
+    const TB* Bt = B + ti.bB;
+    const uint32_t sb = stage0 + (uint32_t)stage * sbytes;
+    const uint32_t sbB = sb + a_bytes;
     if constexpr (REG) {
 #pragma unroll
       for (int u = 0; u < kRegVec; ++u) {
         const int i = tid + u * kThreads;
-        if (i < nvA)
-          cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu) * (uint32_t)sizeof(TA),
-                                    At + rA[u]);
+        if (i < nvA) cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu), At + rA[u]);
         if (BETA && i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
       }
     } else {
+      const int LA = d.LA, LB = d.LB, padA = d.padA;
+      const FastDiv divLA = d.divLA, divLB = d.divLB, divSig = d.divSigmaA;
       for (int i = tid; i < nvA; i += kThreads) {
         const int p = i * VA;
         const int s = (int)fdiv((uint32_t)p, divLA);
@@ -591,13 +624,14 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
     }
   };
 
-  auto out_vec = [&](const TA* st, const TB* sB, int q, const uint16_t* pos, TB* dst) {
+  // one B vector: gather VB staged elements (byte offsets from the stage base), scale, combine, store
+  auto out_vec = [&](const unsigned char* stage, const TB* sB, int q, const uint32_t* off, TB* dst) {
     Vec<TB, VB> out;
     Vec<TB, VB> bv;
     if (BETA) bv = *reinterpret_cast<const Vec<TB, VB>*>(sB + q);
 #pragma unroll
     for (int j = 0; j < VB; ++j) {
-      const TA tj = scale_a(alpha, st[pos[j]]);
+      const TA tj = scale_a(alpha, *reinterpret_cast<const TA*>(stage + off[j]));
       if (BETA)
         out.v[j] = combine<TA, TB>(tj, bv.v[j], beta);
       else
@@ -605,48 +639,51 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
     }
     st_vec<TB, VB>(dst, out, STREAM);
   };
-  auto reg_pos_of = [&](int u, uint16_t* pos) {
+  auto reg_pos_of = [&](int u, uint32_t* off) {
 #pragma unroll
     for (int j = 0; j < VB; ++j) {
       const int e = u * VB + j;
-      pos[j] = (uint16_t)((e & 1) ? (gp[e >> 1] >> 16) : (gp[e >> 1] & 0xffffu));
+      off[j] = (e & 1) ? (gp[e >> 1] >> 16) : (gp[e >> 1] & 0xffffu);
     }
   };
 
-  for (int k = 0; k < S - 1; ++k) {
-    issue(blockIdx.x + k * G, k);
+  if (tid == 0)
+    for (int j = 0; j < S; ++j) decode_into(blockIdx.x + j * G, info[j]);
+  __syncthreads();
+  for (int j = 0; j < S - 1; ++j) {
+    issue(info[j], j);
     cp_async_commit();
   }
   int cur = 0;  // ring slot of tile k; the slot S - 1 ahead is the one before it
   for (uint32_t k = 0;; ++k) {
     const uint32_t t = blockIdx.x + k * G;
     if (t >= ntiles) break;
-    issue(t + (S - 1) * G, cur == 0 ? S - 1 : cur - 1);
+    issue(info[(k + S - 1) & 3], cur == 0 ? S - 1 : cur - 1);
     cp_async_commit();
-    int64_t bA, bB;
-    int lim[2];
-    const bool full = decode_tile(d, t, bA, bB, lim);
-    TB* Bt = B + bB;
-    unsigned char* stage = smem_raw + cur * sbytes;
-    TA* st = reinterpret_cast<TA*>(stage);
-    const TB* sB = reinterpret_cast<const TB*>(stage + a_bytes);
     if (S == 3)
       cp_async_wait<2>();
     else
       cp_async_wait<1>();
     __syncthreads();
-    if (full) {
+    if (tid == 0) decode_into(t + S * G, info[(k + S) & 3]);
+    const TileInfo& ti = info[k & 3];
+    TB* Bt = B + ti.bB;
+    const unsigned char* stage = smem_raw + cur * sbytes;
+    const TB* sB = reinterpret_cast<const TB*>(stage + a_bytes);
+    if (ti.state == 1) {
       if constexpr (REG) {
 #pragma unroll
         for (int u = 0; u < kRegVec; ++u) {
           const int i = tid + u * kThreads;
           if (i < nvB) {
-            uint16_t pos[VB];
-            reg_pos_of(u, pos);
-            out_vec(st, sB, i * VB, pos, Bt + rB[u]);
+            uint32_t off[VB];
+            reg_pos_of(u, off);
+            out_vec(stage, sB, i * VB, off, Bt + rB[u]);
           }
         }
       } else {
+        const int LB = d.LB;
+        const FastDiv divLB = d.divLB;
         if (reg_pos) {
 #pragma unroll
           for (int u = 0; u < kVecB; ++u) {
@@ -654,9 +691,11 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
             if (i < nvB) {
               const int q = i * VB;
               const int s = (int)fdiv((uint32_t)q, divLB);
-              uint16_t pos[VB];
-              reg_pos_of(u, pos);
-              out_vec(st, sB, q, pos, Bt + (segB[s] + (q - s * LB)));
+              uint32_t off[VB];
+              reg_pos_of(u, off);
+#pragma unroll
+              for (int j = 0; j < VB; ++j) off[j] *= (uint32_t)sizeof(TA);
+              out_vec(stage, sB, q, off, Bt + (segB[s] + (q - s * LB)));
             }
           }
         } else {
@@ -665,12 +704,19 @@ __global__ void __launch_bounds__(kThreads, 4) tile_async_kernel(const TileDesc*
             const int s = (int)fdiv((uint32_t)q, divLB);
             uint16_t pos[VB];
             ld_u16s<TA, VB>(gtab + q, pos);
-            out_vec(st, sB, q, pos, Bt + (segB[s] + (q - s * LB)));
+            uint32_t off[VB];
+#pragma unroll
+            for (int j = 0; j < VB; ++j) off[j] = (uint32_t)pos[j] * (uint32_t)sizeof(TA);
+            out_vec(stage, sB, q, off, Bt + (segB[s] + (q - s * LB)));
           }
         }
       }
     } else {
-      tile_ragged_call<TA, TB, BETA, STREAM>(d, tg, lim[0], lim[1], A + bA, Bt, alpha, beta, st);
+      const TileTables tg{reinterpret_cast<const int64_t*>(base + d.off_segA),
+                          reinterpret_cast<const int64_t*>(base + d.off_segB),
+                          reinterpret_cast<const uint16_t*>(base + d.off_perm)};
+      tile_ragged_call<TA, TB, BETA, STREAM>(d, tg, ti.lim0, ti.lim1, A + ti.bA, Bt, alpha, beta,
+                                             reinterpret_cast<TA*>(smem_raw + cur * sbytes));
     }
     __syncthreads();
     cur = cur + 1 == S ? 0 : cur + 1;

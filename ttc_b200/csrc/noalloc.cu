@@ -106,7 +106,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   int va = p.vecA, vb = p.vecB;
   while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
   while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
-  const bool reg = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
+  const bool reg = td->reg_ok && td->P / va <= 1024 && td->P / vb <= 1024;
   const int kernel = reg ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
   const int variant = p.beta_nonzero ? 2 : (p.streaming ? 1 : 0);
   ttcb::KernelRef k = ttcb::pick_kernel(p.ta, p.tb, kernel, va, vb, variant);

@@ -527,6 +527,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
+    td.reg_ok = (td.fast && td.stage_elems * (int64_t)EA < 65536 && P * (int64_t)EB < 65536) ? 1 : 0;
   }
 
   p->host_desc.assign(off, 0);
