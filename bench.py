@@ -366,19 +366,27 @@ def run_e2e(args, items, stream, dev, world):
     d2h = sum(hB.numel() * hB.element_size() for _, hB in host)
     outs = [torch.empty_like(hB, pin_memory=True) for _, hB in host]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    out_done = [None] * len(sub)  # per case: its last copy-out, before its buffers are refilled
 
     def one():
-        for (c, plan, A, B), (hA, hB), o in zip(sub, host, outs):
+        for k, ((c, plan, A, B), (hA, hB), o) in enumerate(zip(sub, host, outs)):
             with torch.cuda.stream(s_in):
-                s_in.wait_stream(s_out)  # the previous step's copy-out of this B is done
+                if out_done[k] is not None:
+                    s_in.wait_event(out_done[k])
                 A.copy_(hA, non_blocking=True)
                 if c["beta"] != 0:
                     B.copy_(hB, non_blocking=True)
-            stream.wait_stream(s_in)
+                ev_in = torch.cuda.Event()
+                ev_in.record(s_in)
+            stream.wait_event(ev_in)
             plan(A, B, c["alpha"], c["beta"], stream)
-            s_out.wait_stream(stream)
+            ev_k = torch.cuda.Event()
+            ev_k.record(stream)
             with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_k)
                 o.copy_(B, non_blocking=True)
+                out_done[k] = torch.cuda.Event()
+                out_done[k].record(s_out)
         stream.wait_stream(s_out)
 
     one()

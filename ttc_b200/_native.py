@@ -82,6 +82,9 @@ TEST_SYMBOLS = [
     ("ttcb_test_plan_host_desc", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_int, ctypes.POINTER(Tuning), _IP, _P, ctypes.c_size_t]),
     ("ttcb_test_desc_layout", None, [_I64P]),
+    ("ttcb_test_plan_shapes", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_int, ctypes.c_char_p,
+                                                ctypes.c_size_t]),
 ]
 
 

@@ -18,7 +18,7 @@ import time
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
-from .core import ELEM_BYTES, Plan, plan_host_json, split_dtype
+from .core import ELEM_BYTES, Plan, plan_shapes, split_dtype
 
 SMS = 148
 L2_BYTES = 126 * 1024 * 1024
@@ -81,14 +81,15 @@ def plan_signature(desc: dict) -> tuple:
 
 
 def tile_shapes(p: Problem, space: Optional[dict] = None) -> list[tuple[dict, dict]]:
-    """Distinct plans the shape knobs (tile_elems x run_bytes) produce: [(shape knobs, plan json)]."""
+    """Distinct plans the shape knobs (tile_elems x run_bytes) produce: [(shape knobs, shape-only
+    plan json)], all planned in one host call without descriptor tables."""
     space = space or knob_space(p.dtype)
+    tunings = [{k: v for k, v in (("tile_elems", te), ("run_bytes", rb)) if v}
+               for te, rb in itertools.product(space["tile_elems"], space["run_bytes"])]
+    descs = plan_shapes(p.perm, p.size, p.dtype, p.beta_nonzero, p.lda, p.ldb, tunings)
     seen = {}
-    for te, rb in itertools.product(space["tile_elems"], space["run_bytes"]):
-        tu = {k: v for k, v in (("tile_elems", te), ("run_bytes", rb)) if v}
-        try:
-            desc = plan_host_json(p.perm, p.size, p.dtype, p.beta_nonzero, p.lda, p.ldb, tu or None)
-        except Exception:
+    for tu, desc in zip(tunings, descs):
+        if desc is None:
             continue
         sig = plan_signature(desc)
         if sig not in seen:

@@ -170,6 +170,25 @@ def plan_host_json(perm, size, dtype="s", beta_nonzero=False, lda=None, ldb=None
     return json.loads(buf.value.decode())
 
 
+def plan_shapes(perm, size, dtype="s", beta_nonzero=False, lda=None, ldb=None, tunings=()) -> list:
+    """Shape-only plans (kernel, tile extents, access widths, cost estimate; no descriptor tables)
+    of one problem under several tunings, in one host call. None where a tuning does not plan."""
+    ta, tb = split_dtype(dtype)
+    n = len(tunings)
+    if n == 0:
+        return []
+    arr = (Tuning * n)(*[Tuning.make(**(t or {})) for t in tunings])
+    args = (len(size), i32(perm), i64(size), i64(lda) if lda else None, i64(ldb) if ldb else None,
+            _native.DTYPES[ta], _native.DTYPES[tb], int(bool(beta_nonzero)), arr, n)
+    size_guess = 1024 * n
+    buf = ctypes.create_string_buffer(size_guess)
+    need = lib().ttcb_test_plan_shapes(*args, buf, size_guess)
+    if need > size_guess:
+        buf = ctypes.create_string_buffer(need)
+        lib().ttcb_test_plan_shapes(*args, buf, need)
+    return json.loads(buf.value.decode())
+
+
 def fuse(perm, size, strideA, strideB):
     """The library's index fusion (host only): returns (perm, size, strideA, strideB)."""
     r = len(size)

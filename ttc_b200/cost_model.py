@@ -7,7 +7,9 @@ when the model is confident, otherwise the top-k predictions are measured (a sho
 
 Features: rank, the permutation as one-hot, log2 extents, log2 strides of A and B, element sizes,
 beta != 0, and the candidate's tile (size, run lengths), access widths, tile kernel variant, grid
-raster order and CTA count, plus the planner's own cost estimate.
+raster order and CTA count (with the grid's waves and the strides between consecutive tiles), plus
+the planner's own cost estimate. Candidates are described by shape-only plans (no descriptor
+tables), so featurising a problem's candidates costs one host call.
 
 The network is trained on the GPU with the library's own kernels (include/ttcb200_mlp.h: tiled GEMM
 with fused bias/ReLU, ReLU backward, column sums, MSE, Adam) on timings the measured search itself
@@ -28,11 +30,11 @@ import numpy as np
 
 from . import _native
 from .autotune import Problem, candidate_tunings, measure, Bench
-from .core import ELEM_BYTES, split_dtype
+from .core import ELEM_BYTES, plan_shapes, split_dtype
 
 MAXD = 6
 DEFAULT_MODEL = Path(__file__).resolve().parent / "data" / "cost_model.npz"
-VERSION = "ttcb-mlp-v1"
+VERSION = "ttcb-mlp-v2"
 
 
 # ------------------------------------------------------------------------------------------------
@@ -88,8 +90,45 @@ def candidate_features(p: Problem, tuning: dict, desc: dict) -> list[float]:
          1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
          1.0 if bl == 0 else 0.0, bl / 444.0,
          min(desc["est_cost"], 200.0) / 32.0, math.log2(max(nt, 1)) / 25.0,
-         float(t.get("fast", 0)), float(t.get("async", 0)), float(t.get("stages", 0)) / 3.0]
+         float(t.get("fast", 0))]
+    # waves of the grid (CTAs: the knob, else about four resident per SM) and the last wave's fill
+    ctas = bl if bl else 4 * 148
+    waves = nt / ctas
+    f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves),
+          math.log2(max(P * ELEM_BYTES[ta], 1)) / 16.0,
+          math.log2(max(P / max(LA, 1), 1)) / 10.0, math.log2(max(P / max(LB, 1), 1)) / 10.0]
+    # the raster: strides (bytes) between consecutive tiles along the fastest grid dimension
+    fu = desc["fused"]
+    ext = t.get("ext") or []
+    order = list(range(fu["rank"]))
+    if lo == 1:
+        order = list(fu["perm"])
+    elif lo == 2:
+        order = order[::-1]
+    jA = jB = 0.0
+    for dd in order:
+        e = ext[dd] if dd < len(ext) else 0
+        if e and e == fu["size"][dd]:
+            continue  # the whole dimension is inside the tile
+        step = e if e else 1
+        jA = math.log2(max(step * fu["strideA"][dd] * ELEM_BYTES[ta], 1)) / 40.0
+        jB = math.log2(max(step * fu["strideB"][dd] * ELEM_BYTES[tb], 1)) / 40.0
+        break
+    f += [jA, jB]
     return f
+
+
+def corpus_features(meta: dict) -> tuple[np.ndarray, np.ndarray]:
+    """Recomputes the feature rows of a stored corpus from its cases and candidate tunings (shape-only
+    planning on the host), so feature changes need no new measurements. Returns (X, case index)."""
+    rows, case = [], []
+    for c, tunings in zip(meta["cases"], meta["tunings"]):
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        descs = plan_shapes(p.perm, p.size, p.dtype, p.beta_nonzero, p.lda, p.ldb, tunings)
+        X = features(p, list(zip(tunings, descs)))
+        rows.append(X)
+        case += [int(c["index"])] * len(X)
+    return np.concatenate(rows).astype(np.float32), np.asarray(case, np.int32)
 
 
 def features(p: Problem, cands) -> np.ndarray:
@@ -335,9 +374,11 @@ def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, v
 
 
 # ------------------------------------------------------------------------------------------------
-def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log=print) -> None:
+def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log=print,
+            deadline: Optional[float] = None) -> bool:
     """Exhaustive measured search over each case's candidates; stores features, log(GB/s), the
-    search wall time, resumable per case (rows of finished cases are kept)."""
+    search wall time, resumable per case (rows of finished cases are kept). Stops early, keeping
+    what it has, once time.time() passes `deadline`; returns True when every case is done."""
     import torch
     done = {}
     if out.exists():
@@ -351,6 +392,9 @@ def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log
     for k, c in enumerate(cases):
         if k in finished:
             continue
+        if deadline is not None and time.time() > deadline:
+            _save_corpus(out, done)
+            return False
         p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
         t0 = time.perf_counter()
         cands = candidate_tunings(p, max_impl, with_desc=True)
@@ -374,11 +418,12 @@ def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log
             if log:
                 log(f"collected {k + 1}/{len(cases)} cases, {len(done['y'])} rows")
     _save_corpus(out, done)
+    return True
 
 
 def _save_corpus(out: Path, d: dict):
     out.parent.mkdir(parents=True, exist_ok=True)
-    np.savez(out, X=np.asarray(d["X"], np.float32), y=np.asarray(d["y"], np.float32),
+    np.savez_compressed(out, X=np.asarray(d["X"], np.float32), y=np.asarray(d["y"], np.float32),
              case=np.asarray(d["case"], np.int32), cand=np.asarray(d["cand"], np.int32),
              search_s=np.asarray(d["search_s"], np.float64),
              meta=np.frombuffer(json.dumps(d["meta"]).encode(), np.uint8))
@@ -442,18 +487,21 @@ def main(argv=None):
     ap.add_argument("cmd", choices=["collect", "train", "evaluate"])
     ap.add_argument("--train-cases", type=int, default=2000)
     ap.add_argument("--test-cases", type=int, default=500)
-    ap.add_argument("--corpus", default="gpurun_out/cost_corpus")
+    ap.add_argument("--corpus", default=str(Path(__file__).resolve().parent / "data" / "cost_corpus"),
+                    help="corpus path prefix (<prefix>_train.npz, <prefix>_test.npz)")
     ap.add_argument("--model", default=str(DEFAULT_MODEL))
     ap.add_argument("--max-impl", type=int, default=64)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--threshold", type=float, default=0.35)
     ap.add_argument("--out-json", default=None)
+    ap.add_argument("--max-seconds", type=float, default=None, help="collect: stop (resumably) after this long")
     a = ap.parse_args(argv)
     train_path = Path(a.corpus + "_train.npz")
     test_path = Path(a.corpus + "_test.npz")
     if a.cmd == "collect":
-        collect(wl.learning_cases(11, a.train_cases), train_path, a.max_impl)
-        collect(wl.learning_cases(12345, a.test_cases), test_path, a.max_impl)
+        deadline = time.time() + a.max_seconds if a.max_seconds else None
+        if collect(wl.learning_cases(11, a.train_cases), train_path, a.max_impl, deadline=deadline):
+            collect(wl.learning_cases(12345, a.test_cases), test_path, a.max_impl, deadline=deadline)
     elif a.cmd == "train":
         z = np.load(train_path)
         m = train(z["X"], z["y"], epochs=a.epochs)

@@ -53,9 +53,9 @@ static ttcb_status cuda_fail(cudaError_t e, const char* what) {
 
 static int variant_of(const ttcb_plan* p) { return p->beta_nonzero ? 2 : (p->streaming ? 1 : 0); }
 
-// Kernels whose shared memory (dynamic, plus the staged kernel's static copy of the descriptor
-// header) may exceed the 48 KB default get the opt-in once per device.
-static bool needs_large_smem(int dynamic_smem) { return dynamic_smem + (int)sizeof(TileDesc) > 48 * 1024; }
+// Kernels whose shared memory (dynamic, plus the staged kernel's static descriptor header and tile
+// ring) may exceed the 48 KB default get the opt-in once per device.
+static bool needs_large_smem(int dynamic_smem) { return dynamic_smem + (int)ttcb::kAsyncStaticSmem > 48 * 1024; }
 
 static void allow_large_smem(const void* func) {
   static std::mutex mu;
@@ -272,6 +272,42 @@ int ttcb_test_fuse(int rank, const int* perm, const int64_t* n, const int64_t* s
 }
 
 // Builds the host part of a plan (no CUDA calls) and returns its JSON description.
+size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                             int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tunings, int n, char* buf,
+                             size_t len) {
+  std::string js = "[";
+  for (int k = 0; k < n; ++k) {
+    ttcb_plan p;
+    p.shape_only = true;
+    bool ok = rank >= 1 && rank <= TTCB_MAX_RANK;
+    for (int j = 0; ok && j < rank; ++j) ok = perm[j] >= 0 && perm[j] < rank;
+    if (ok) {
+      p.rank = rank;
+      for (int i = 0; i < rank; ++i) {
+        p.perm[i] = perm[i];
+        p.size[i] = size[i];
+        p.lda[i] = lda ? lda[i] : size[i];
+      }
+      for (int j = 0; j < rank; ++j) p.ldb[j] = ldb ? ldb[j] : size[perm[j]];
+      p.ta = (ttcb_dtype)type_a;
+      p.tb = (ttcb_dtype)type_b;
+      p.beta_nonzero = beta_nonzero;
+      if (tunings) p.tuning = tunings[k];
+      std::string err;
+      ok = plan_build_host(&p, err) == TTCB_OK;
+    }
+    js += (k ? "," : "");
+    js += ok ? plan_describe_json(&p) : std::string("null");
+  }
+  js += "]";
+  if (buf && len) {
+    size_t m = std::min(len - 1, js.size());
+    std::memcpy(buf, js.data(), m);
+    buf[m] = 0;
+  }
+  return js.size() + 1;
+}
+
 int ttcb_test_plan_host(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
                         int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len) {
   ttcb_plan p;

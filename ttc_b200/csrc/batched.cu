@@ -47,7 +47,9 @@ struct ttcb_batch {
   int64_t bytes = 0;
   unsigned long long total = 0;
   int blocks = 0;
-  int smem = 0;
+  int smem = 0;         // tile buffer + the largest problem's tables
+  int slots_bytes = 0;  // tile buffer (the tables follow it)
+  int chunk = 1;        // items claimed per atomic
   void* d_probs = nullptr;
   int64_t* d_prefix = nullptr;
   unsigned char* d_desc = nullptr;
@@ -132,7 +134,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
   std::vector<unsigned char> hdesc(std::max<int64_t>(desc_bytes, 16), 0);
   std::vector<ttcb::BatchProblem> hp(count);
   std::vector<int64_t> prefix(count + 1, 0);
-  int max_slots_bytes = 0;
+  int max_slots_bytes = 0, max_table_bytes = 0;
   for (int i = 0; i < count; ++i) {
     const ttcb_plan* p = plans[i];
     ttcb::BatchProblem& q = hp[i];
@@ -159,13 +161,15 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
         const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
         items = td->ntiles;
         max_slots_bytes = std::max<int>(max_slots_bytes, (int)ttcb::tile_slots_bytes(td->phys_size, EA));
+        max_table_bytes = std::max<int>(max_table_bytes, 8 * (td->nsegA + td->nsegB) + 4 * ((td->P + 1) / 2));
       }
       b->bytes += ttcb_plan_bytes(p);
     }
     prefix[i + 1] = prefix[i] + items;
   }
   b->total = (unsigned long long)prefix[count];
-  b->smem = max_slots_bytes;
+  b->slots_bytes = (int)((max_slots_bytes + 15) & ~15);
+  b->smem = b->slots_bytes + max_table_bytes;
 
   // device copies
   if ((e = cudaMalloc(&b->d_desc, hdesc.size())) != cudaSuccess ||
@@ -193,7 +197,8 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
     batch_free(b);
     return bfail(TTCB_ERR_DTYPE, "no batched kernel for this type pair");
   }
-  if (b->smem > 48 * 1024) cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (b->smem + (int)sizeof(TileDesc) + 64 > 48 * 1024)  // + its static header copy, item and problem index
+    cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, b->smem);
@@ -205,6 +210,9 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
   int64_t nb = blocks > 0 ? blocks : resident;
   nb = std::min<int64_t>(nb, std::max<unsigned long long>(b->total, 1ull));
   b->blocks = (int)std::max<int64_t>(nb, 1);
+  // about sixteen claims per CTA keep the tail balanced while amortising the claim and its search
+  b->chunk = (int)std::max<unsigned long long>(1ull, std::min<unsigned long long>(
+                                                         32ull, b->total / (16ull * (unsigned long long)b->blocks)));
   *out = b;
   return TTCB_OK;
 }
@@ -215,7 +223,8 @@ static ttcb_status batch_enqueue(ttcb_batch* b, cudaStream_t s) {
   if (b->total == 0) return TTCB_OK;
   ttcb::BatchKernelRef k = ttcb::pick_batch_kernel(b->ta, b->tb, batch_variant(b));
   e = k.fn(b->d_probs, b->d_prefix, b->count, b->total, b->d_counter,
-           reinterpret_cast<int*>(b->d_counter + 1), b->alpha, b->beta, b->blocks, b->smem, s);
+           reinterpret_cast<int*>(b->d_counter + 1), b->alpha, b->beta, b->blocks, b->smem, b->slots_bytes,
+           b->chunk, s);
   if (e != cudaSuccess) return bcuda(e, "batched kernel launch");
   return TTCB_OK;
 }

@@ -485,6 +485,10 @@ struct TileInfo {
   int32_t lim0, lim1, pad_;
 };
 
+// Static shared memory of the staged kernel (descriptor header + tile ring), on top of its dynamic
+// shared memory.
+constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + 4 * sizeof(TileInfo);
+
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
 // vectors per thread and side whose offsets fit 32 bits and whose staged bytes fit 16 bits): A
 // source offsets rA, staged byte offsets dA (two per register), B offsets rB, gather byte offsets
@@ -498,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
-  __shared__ TileInfo info[4];
+  __shared__ TileInfo info[4];  // kAsyncStaticSmem counts both
   const int tid = threadIdx.x;
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
     reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];

@@ -199,14 +199,14 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
 template <bool BETA, bool STREAM>
 static cudaError_t launch_batch(const void* probs, const int64_t* prefix, int count, unsigned long long total,
                                 unsigned long long* counter, int* status, const void* alpha, const void* beta,
-                                int blocks, int smem, cudaStream_t stream) {
+                                int blocks, int smem, int slots_bytes, int chunk, cudaStream_t stream) {
   TA al;
   std::memcpy(&al, alpha, sizeof(TA));
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
   batch_kernel<TA, TB, BETA, STREAM><<<blocks, kThreads, smem, stream>>>(
-      static_cast<const BatchProblem*>(probs), prefix, count, total, counter, status, al, be);
+      static_cast<const BatchProblem*>(probs), prefix, count, total, counter, status, al, be, slots_bytes, chunk);
   return cudaGetLastError();
 }
 

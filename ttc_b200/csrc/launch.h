@@ -21,7 +21,7 @@ KernelRef pick_kernel(ttcb_dtype ta, ttcb_dtype tb, int kernel, int va, int vb, 
 
 using BatchLaunchFn = cudaError_t (*)(const void* probs, const int64_t* prefix, int count, unsigned long long total,
                                       unsigned long long* counter, int* status, const void* alpha, const void* beta,
-                                      int blocks, int smem, cudaStream_t stream);
+                                      int blocks, int smem, int slots_bytes, int chunk, cudaStream_t stream);
 struct BatchKernelRef {
   BatchLaunchFn fn = nullptr;
   const void* func = nullptr;

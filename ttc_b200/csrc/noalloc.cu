@@ -111,7 +111,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   const int variant = p.beta_nonzero ? 2 : (p.streaming ? 1 : 0);
   ttcb::KernelRef k = ttcb::pick_kernel(p.ta, p.tb, kernel, va, vb, variant);
   if (!k.fn) return na_fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (p.smem_async + (int)sizeof(TileDesc) > 48 * 1024) {
+  if (p.smem_async + (int)ttcb::kAsyncStaticSmem > 48 * 1024) {
     e = cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_async);
     if (e != cudaSuccess) return na_cuda(e, "cudaFuncSetAttribute");
   }

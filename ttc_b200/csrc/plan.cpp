@@ -416,8 +416,15 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       for (int64_t m = 1; m <= 8; m *= 2)
         if (tsA[d] > 1 && m * tsA[d] < P && (m * tsA[d]) % c.vecA == 0) sigmas.push_back(m * tsA[d]);
     for (int64_t k = c.vecA; k <= 64 && k < P; k += c.vecA) sigmas.push_back(k);
+    // one wavefront per lane group and load is the floor; stop searching once it is reached
+    int64_t ideal = 0;
+    for (int w = 0; w < 4; ++w)
+      for (int j = 0; j < c.vecB; ++j)
+        for (int g0 = 0; g0 < 32; g0 += group)
+          if (((int64_t)w * 32 + g0) * c.vecB < P) ++ideal;
     int64_t best_cost = -1, best_sigma = c.LA, best_pad = 0;
     for (int64_t sg : sigmas) {
+      if (best_cost == ideal) break;
       sigma = sg;
       for (int k = 0; k <= 8; ++k) {
         const int64_t cand = (int64_t)k * c.vecA;
@@ -429,6 +436,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
           best_sigma = sg;
           best_pad = cand;
         }
+        if (best_cost == ideal) break;
       }
     }
     sigma = best_sigma;
@@ -706,9 +714,9 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   }
   p->kernel = kernel;
   if (kernel == TTCB_KERNEL_ROW) return build_row_desc(p, err);
+  int64_t ntiles = 1;
   {
     // tile counts must fit the kernels' 32-bit tile index
-    int64_t ntiles = 1;
     for (int d = 0; d < f.rank; ++d) {
       int64_t e = best.ext[d] > 0 ? best.ext[d] : 1;
       if (best.ext[d] > 0 && best.ext[d] == f.n[d]) continue;
@@ -718,6 +726,17 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
         return TTCB_ERR_UNSUPPORTED;
       }
     }
+  }
+  p->tile_P = best.P;
+  p->tile_LA = best.LA;
+  p->tile_LB = best.LB;
+  p->tile_ntiles = ntiles;
+  for (int d = 0; d < f.rank; ++d) p->tile_ext[d] = best.ext[d];
+  if (p->shape_only) {
+    p->vecA = best.vecA;
+    p->vecB = best.vecB;
+    p->est_cost = best.cost;
+    return TTCB_OK;
   }
   build_tile_desc(p, best, EA);
   return TTCB_OK;
@@ -747,7 +766,15 @@ std::string plan_describe_json(const ttcb_plan* p) {
     o << ",\"tile\":{\"P\":" << t->P << ",\"LA\":" << t->LA << ",\"LB\":" << t->LB << ",\"ntiles\":" << t->ntiles
       << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
-      << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages << "}";
+      << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages << ",\"ext\":[";
+    for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
+    o << "]}";
+  } else if (p->kernel == TTCB_KERNEL_TILE && p->shape_only) {
+    const bool fits = p->tile_P / p->vecA <= 1024 && p->tile_P / p->vecB <= 1024;
+    o << ",\"tile\":{\"P\":" << p->tile_P << ",\"LA\":" << p->tile_LA << ",\"LB\":" << p->tile_LB
+      << ",\"ntiles\":" << p->tile_ntiles << ",\"fast\":" << (fits ? 1 : 0) << ",\"shape_only\":1,\"ext\":[";
+    for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
+    o << "]}";
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     o << ",\"row\":{\"w\":" << rd->w << ",\"chunk\":" << rd->chunk << ",\"units\":" << rd->nunits << "}";

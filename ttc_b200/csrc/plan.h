@@ -47,6 +47,12 @@ struct ttcb_plan {
   int smem_async = 0;     // staged tile kernel (stages + tables)
   int blocks_async = 0;   // CTAs for the staged tile kernel
   int device = 0;
+
+  // shape-only planning (candidate features for the learned selector): the tile choice without
+  // descriptor tables
+  bool shape_only = false;
+  int64_t tile_P = 0, tile_LA = 0, tile_LB = 0, tile_ntiles = 0;
+  int64_t tile_ext[TTCB_MAXR] = {0};  // tile extent per fused dimension (0 = not in the tile)
 };
 
 // Fills everything except dev_desc / blocks (which need the CUDA device). Returns a status and a

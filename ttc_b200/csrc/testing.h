@@ -16,4 +16,10 @@ size_t ttcb_test_plan_host_desc(int rank, const int* perm, const int64_t* size, 
                                 const int64_t* ldb, int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning,
                                 int* kernel, void* buf, size_t len);
 void ttcb_test_desc_layout(int64_t* out);
+// Shape-only plans of one problem under n tunings (the learned selector's candidate features):
+// writes a JSON array (one plan description per tuning, null where planning failed) into buf and
+// returns the length it needs including the terminator.
+size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                             int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tunings, int n, char* buf,
+                             size_t len);
 }
