@@ -49,9 +49,12 @@ def parse():
     ap.add_argument("--cpu-sample-cases", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case"],
                     help="sweep: the 64-case 200 MiB sweep (default); batched: 4096 small transpositions "
-                         "in one persistent launch against per-call launches")
+                         "in one persistent launch against per-call launches; case: one sweep case run "
+                         "--reps times with its default plan (a small command for profilers)")
+    ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
+    ap.add_argument("--reps", type=int, default=3, help="case: launches")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-tuning", default="search", choices=["search", "default"],
                     help="per-problem schedules: measured search (the autotuner) or the planner default")
@@ -227,6 +230,8 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.workload == "batched":
         return run_batched(args, rank, world, local)
+    if args.workload == "case":
+        return run_case(args)
 
     import torch
     import torch.distributed as dist
@@ -414,6 +419,34 @@ def run_e2e(args, items, stream, dev, world):
             "d2h_bytes_per_step": d2h, "cases": len(sub), "ms_per_step": round(ms, 3),
             "note": ("pinned host A (and B when beta != 0) copied in and B copied out for every case inside the "
                      "timed region; copy-in and copy-out on separate streams (PCIe both directions)")}
+
+
+def run_case(args):
+    """One sweep case, `--reps` launches of its default plan on seeded resident inputs; prints the
+    plan and the mean GB/s (CUDA events). Meant to sit under a profiler."""
+    import torch
+    import ttc_b200.workloads as wl
+    from ttc_b200 import Plan
+    c = wl.sweep_cases(args.seed)[args.case]
+    tmap = {"s": torch.float32, "d": torch.float64}
+    n = math.prod(c["size"])
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(c["seed"])
+    A = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen)
+    B = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen)
+    plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.reps):
+        plan(A, B, c["alpha"], c["beta"])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.reps, 1)
+    print(json.dumps({"case": args.case, "perm": c["perm"], "size": c["size"], "dtype": c["dtype"],
+                      "beta": c["beta"], "GBps": round(plan.bytes / (ms / 1e3) / 1e9, 1), "bytes": plan.bytes,
+                      "plan": plan.describe()}), flush=True)
+    plan.close()
+    return 0
 
 
 # ------------------------------------------------------------------------------------------------

@@ -94,3 +94,22 @@ def test_training_fits_a_smooth_function():
     y = (np.sin(2 * X[:, 0]) + X[:, 1] * X[:, 2] + 0.5 * X[:, 3] ** 2).astype(np.float32)
     m = train(X, y, epochs=60, lr=3e-3, batch=512, log=None)
     assert m.rmse < 0.15 * float(np.std(y)), (m.rmse, float(np.std(y)))
+
+
+def test_trained_selector_beats_the_planner_default():
+    """What the trained network gains over the method without it, on the 500 held-out problems
+    whose every candidate schedule was timed: the network's top-1 schedule keeps a larger share of
+    the best measured GB/s than the planner's own default schedule. Inference runs on the GPU
+    with the library's kernels."""
+    import json
+    from ttc_b200.cost_model import DEFAULT_MODEL, MLP, corpus_features, stored_selection
+    corpus = DEFAULT_MODEL.parent / "cost_corpus_test.npz"
+    z = np.load(corpus)
+    meta = json.loads(bytes(z["meta"]).decode())
+    X, case = corpus_features(meta)
+    assert np.array_equal(case, z["case"])
+    m = MLP.load(DEFAULT_MODEL)
+    r = stored_selection(m.predict(X), z["y"], case, meta, m.rmse, threshold=0.0, topk=1)
+    assert r["cases"] == 500
+    assert r["top1_over_best"] >= r["default_over_best"] + 0.01, r
+    assert r["top1_over_best"] >= 0.92, r

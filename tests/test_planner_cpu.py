@@ -160,3 +160,30 @@ def test_planner_choices_for_reference_shapes():
     # empty tensors are a no-op plan
     j = plan_host_json([1, 0], [0, 5], "s", False)
     assert j["elements"] == 0
+
+
+def test_shape_only_plans_match_full_plans():
+    """The learned selector plans its candidates shape-only and in one call (tile shapes enumerated
+    once per problem); every candidate must describe the same tile, widths and cost as the full
+    plan that the tuning produces."""
+    import itertools
+    from ttc_b200.core import plan_shapes
+    rng = np.random.default_rng(7)
+    tunings = [{k: v for k, v in (("tile_elems", te), ("run_bytes", rb), ("vec", vec)) if v}
+               for te, rb, vec in itertools.product([0, 512, 2048, 8192], [0, 128, 1024], [0, 1])]
+    for it in range(60):
+        perm, size, lda, ldb = _random_problem(rng, max_rank=6, max_ext=40)
+        dtype = ["s", "d", "zc", "sd"][it % 4]
+        shapes = plan_shapes(perm, size, dtype, bool(it % 2), lda, ldb, tunings)
+        for tu, sh in zip(tunings, shapes):
+            try:
+                full = plan_host_json(perm, size, dtype, bool(it % 2), lda, ldb, tu)
+            except TTCError:
+                assert sh is None
+                continue
+            assert sh is not None
+            assert (sh["kernel"], sh["vecA"], sh["vecB"]) == (full["kernel"], full["vecA"], full["vecB"])
+            assert abs(sh["est_cost"] - full["est_cost"]) <= 1e-9 * max(1.0, full["est_cost"])
+            if full["kernel"] == "tile":
+                for k in ("P", "LA", "LB", "ntiles", "ext"):
+                    assert sh["tile"][k] == full["tile"][k], (perm, size, dtype, tu, k)

@@ -70,7 +70,9 @@ def problem_features(p: Problem, desc: dict) -> list[float]:
     return f
 
 
-def candidate_features(p: Problem, tuning: dict, desc: dict) -> list[float]:
+def _shape_part(p: Problem, desc: dict) -> tuple:
+    """The features of a candidate that depend only on its plan (tile shape), not on the launch
+    knobs: (static values, tile count, raster jumps (A, B) for loop orders 0, 1, 2)."""
     ta, tb = split_dtype(p.dtype)
     t = desc.get("tile") or {}
     row = desc.get("row") or {}
@@ -79,42 +81,48 @@ def candidate_features(p: Problem, tuning: dict, desc: dict) -> list[float]:
     LA = t.get("LA", row.get("w", 1))
     LB = t.get("LB", row.get("w", 1))
     nt = t.get("ntiles", row.get("units", 1))
-    tv = tuning.get("tile_variant", 0)
-    lo = tuning.get("loop_order", 0)
-    bl = tuning.get("blocks", 0)
-    f = [1.0 if is_tile else 0.0, 0.0 if is_tile else 1.0,
-         math.log2(max(P, 1)) / 14.0, math.log2(max(LA, 1)) / 14.0, math.log2(max(LB, 1)) / 14.0,
-         desc["vecA"] / 4.0, desc["vecB"] / 4.0,
-         math.log2(max(LA * ELEM_BYTES[ta], 1)) / 16.0, math.log2(max(LB * ELEM_BYTES[tb], 1)) / 16.0,
-         1.0 if tv == 0 else 0.0, 1.0 if tv == 2 else 0.0, 1.0 if tv == 1 else 0.0,
-         1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
-         1.0 if bl == 0 else 0.0, bl / 444.0,
-         min(desc["est_cost"], 200.0) / 32.0, math.log2(max(nt, 1)) / 25.0,
-         float(t.get("fast", 0))]
-    # waves of the grid (CTAs: the knob, else about four resident per SM) and the last wave's fill
-    ctas = bl if bl else 4 * 148
-    waves = nt / ctas
-    f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves),
-          math.log2(max(P * ELEM_BYTES[ta], 1)) / 16.0,
-          math.log2(max(P / max(LA, 1), 1)) / 10.0, math.log2(max(P / max(LB, 1), 1)) / 10.0]
+    head = [1.0 if is_tile else 0.0, 0.0 if is_tile else 1.0,
+            math.log2(max(P, 1)) / 14.0, math.log2(max(LA, 1)) / 14.0, math.log2(max(LB, 1)) / 14.0,
+            desc["vecA"] / 4.0, desc["vecB"] / 4.0,
+            math.log2(max(LA * ELEM_BYTES[ta], 1)) / 16.0, math.log2(max(LB * ELEM_BYTES[tb], 1)) / 16.0]
+    mid = [min(desc["est_cost"], 200.0) / 32.0, math.log2(max(nt, 1)) / 25.0, float(t.get("fast", 0))]
+    tail = [math.log2(max(P * ELEM_BYTES[ta], 1)) / 16.0,
+            math.log2(max(P / max(LA, 1), 1)) / 10.0, math.log2(max(P / max(LB, 1), 1)) / 10.0]
     # the raster: strides (bytes) between consecutive tiles along the fastest grid dimension
     fu = desc["fused"]
     ext = t.get("ext") or []
-    order = list(range(fu["rank"]))
-    if lo == 1:
-        order = list(fu["perm"])
-    elif lo == 2:
-        order = order[::-1]
-    jA = jB = 0.0
-    for dd in order:
-        e = ext[dd] if dd < len(ext) else 0
-        if e and e == fu["size"][dd]:
-            continue  # the whole dimension is inside the tile
-        step = e if e else 1
-        jA = math.log2(max(step * fu["strideA"][dd] * ELEM_BYTES[ta], 1)) / 40.0
-        jB = math.log2(max(step * fu["strideB"][dd] * ELEM_BYTES[tb], 1)) / 40.0
-        break
-    f += [jA, jB]
+    jumps = []
+    for lo in (0, 1, 2):
+        order = list(range(fu["rank"]))
+        if lo == 1:
+            order = list(fu["perm"])
+        elif lo == 2:
+            order = order[::-1]
+        jA = jB = 0.0
+        for dd in order:
+            e = ext[dd] if dd < len(ext) else 0
+            if e and e == fu["size"][dd]:
+                continue  # the whole dimension is inside the tile
+            step = e if e else 1
+            jA = math.log2(max(step * fu["strideA"][dd] * ELEM_BYTES[ta], 1)) / 40.0
+            jB = math.log2(max(step * fu["strideB"][dd] * ELEM_BYTES[tb], 1)) / 40.0
+            break
+        jumps.append((jA, jB))
+    return head, mid, tail, nt, jumps
+
+
+def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None) -> list[float]:
+    head, mid, tail, nt, jumps = shape or _shape_part(p, desc)
+    tv = tuning.get("tile_variant", 0)
+    lo = tuning.get("loop_order", 0)
+    bl = tuning.get("blocks", 0)
+    f = head + [1.0 if tv == 0 else 0.0, 1.0 if tv == 2 else 0.0, 1.0 if tv == 1 else 0.0,
+                1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
+                1.0 if bl == 0 else 0.0, bl / 444.0] + mid
+    # waves of the grid (CTAs: the knob, else about four resident per SM) and the last wave's fill
+    waves = nt / (bl if bl else 4 * 148)
+    f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves)] + tail
+    f += list(jumps[lo if lo in (0, 1, 2) else 0])
     return f
 
 
@@ -136,7 +144,14 @@ def features(p: Problem, cands) -> np.ndarray:
     if not cands:
         return np.zeros((0, 0), np.float32)
     pf = problem_features(p, cands[0][1])
-    return np.asarray([pf + candidate_features(p, tu, d) for tu, d in cands], dtype=np.float32)
+    shapes = {}
+    rows = []
+    for tu, d in cands:
+        sh = shapes.get(id(d))
+        if sh is None:
+            sh = shapes[id(d)] = _shape_part(p, d)
+        rows.append(pf + candidate_features(p, tu, d, sh))
+    return np.asarray(rows, dtype=np.float32)
 
 
 # ------------------------------------------------------------------------------------------------
@@ -302,19 +317,27 @@ def numpy_forward_backward(params, X, y):
 
 
 def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batch: int = 2048, seed: int = 0,
-          val: float = 0.1, log=print) -> MLP:
-    """Fits log(GB/s) with the library's kernels; holds out `val` of the problems' rows for RMSE."""
+          val: float = 0.1, log=print, groups: Optional[np.ndarray] = None) -> MLP:
+    """Fits log(GB/s) with the library's kernels. Holds out `val` of the rows for the RMSE (whole
+    problems when `groups` gives each row's problem)."""
     import torch
     rng = np.random.default_rng(seed)
-    idx = rng.permutation(len(X))
-    nval = int(len(X) * val)
-    vi, ti = idx[:nval], idx[nval:]
+    if groups is not None:
+        ug = rng.permutation(np.unique(groups))
+        held = np.isin(groups, ug[: int(len(ug) * val)])
+        vi, ti = np.nonzero(held)[0], rng.permutation(np.nonzero(~held)[0])
+        nval = len(vi)
+    else:
+        idx = rng.permutation(len(X))
+        nval = int(len(X) * val)
+        vi, ti = idx[:nval], idx[nval:]
     m = MLP(X.shape[1], 128, seed)
     m.mu = X[ti].mean(0)
     m.sd = X[ti].std(0) + 1e-6
     m.ymu, m.ysd = float(y[ti].mean()), float(y[ti].std() + 1e-6)
     Xt = m._norm(X[ti])
     yt = torch.from_numpy(((y[ti] - m.ymu) / m.ysd).astype(np.float32)).cuda().reshape(-1, 1)
+    best_vr, best_params = float("inf"), None
     for ep in range(epochs):
         order = torch.from_numpy(rng.permutation(len(ti))).cuda()
         tot = 0.0
@@ -326,11 +349,17 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
             grads = m.backward(d, cache)
             m.step(grads, lr * (0.5 ** (ep // 20)))
             tot += float(loss.item()) * len(sel)
+        if nval:
+            # keep the weights of the epoch with the lowest held-out error (early stopping)
+            vr = float(np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)))
+            if vr < best_vr:
+                best_vr, best_params = vr, [q.clone() for q in m.params]
         if log and (ep % 10 == 0 or ep == epochs - 1):
-            vr = np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)) if nval else float("nan")
-            log(f"epoch {ep}: train mse {tot / len(ti):.4f} (normalised), val rmse {vr:.4f} log(GB/s)")
+            log(f"epoch {ep}: train mse {tot / len(ti):.4f} (normalised), val rmse "
+                f"{vr if nval else float('nan'):.4f} log(GB/s)")
     if nval:
-        m.rmse = float(np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)))
+        m.params = best_params
+        m.rmse = best_vr
     return m
 
 
@@ -354,11 +383,11 @@ def load_default(path: Optional[Path] = None) -> MLP:
 
 
 def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, verify: bool = True,
-           model: Optional[MLP] = None, topk: int = 8, measure_choice: bool = True) -> dict:
+           model: Optional[MLP] = None, topk: int = 2, measure_choice: bool = True) -> dict:
     """Picks a schedule with the model. Below the confidence threshold, measures the top-k
     predictions and keeps the fastest (a short measured search). Returns the measured results."""
     model = model or load_default()
-    thr = 0.35 if confidence is None else confidence
+    thr = 0.1 if confidence is None else confidence
     t0 = time.perf_counter()
     cands = candidate_tunings(p, max_impl, with_desc=True)
     X = features(p, cands)
@@ -429,53 +458,99 @@ def _save_corpus(out: Path, d: dict):
              meta=np.frombuffer(json.dumps(d["meta"]).encode(), np.uint8))
 
 
-def evaluate(model: MLP, corpus: Path, log=print, threshold: float = 0.35, topk: int = 8,
-             time_cases: int = 100) -> dict:
-    """Held-out evaluation from stored exhaustive measurements: model top-1 (or top-k when not
-    confident) GB/s vs the best measured, and the planner default (no model) vs the best. Model
-    selection time is measured on the first `time_cases` problems (candidate planning + features +
-    inference, plus the top-k measurements when it falls back)."""
-    z = np.load(corpus)
-    X, y, case = z["X"], z["y"], z["case"]
-    meta = json.loads(bytes(z["meta"]).decode())
-    search_s = z["search_s"]
-    ratios, default_ratios, fallbacks = [], [], 0
-    pred = model.predict(X)
+def stored_selection(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: dict, rmse: float,
+                     threshold: float, topk: int) -> dict:
+    """Selection quality on stored exhaustive measurements: per problem, the GB/s of the model's
+    top-1 (or best of its top-k when its confidence is below the threshold) and of the planner's
+    default schedule, over the best measured GB/s."""
     index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
+    top1, gated, dflt, fb = [], [], [], []
     for k in np.unique(case):
         rows = np.nonzero(case == k)[0]
         tunings = meta["tunings"][index_of[int(k)]]
-        dflt = tunings.index({}) if {} in tunings else 0
-        best = np.exp(y[rows].max())
-        pk = pred[rows]
-        conf = confidence_of(pk, model.rmse)
-        if conf < threshold:
-            fallbacks += 1
-            top = rows[np.argsort(-pk)[:topk]]
-            chosen = np.exp(y[top].max())
-        else:
-            chosen = np.exp(y[rows[np.argmax(pk)]])
-        ratios.append(chosen / best)
-        default_ratios.append(np.exp(y[rows[dflt]]) / best)  # the planner's default schedule
-    ratios = np.asarray(ratios)
-    default_ratios = np.asarray(default_ratios)
-    # selection time on real problems
-    t_sel, t_search = [], []
+        best = y[rows].max()
+        order = np.argsort(-pred[rows])
+        top1.append(np.exp(y[rows[order[0]]] - best))
+        low = confidence_of(pred[rows], rmse) < threshold
+        fb.append(low)
+        gated.append(np.exp(y[rows[order[:topk]]].max() - best) if low else top1[-1])
+        d = tunings.index({}) if {} in tunings else 0
+        dflt.append(np.exp(y[rows[d]] - best))
+    top1, gated, dflt = map(np.asarray, (top1, gated, dflt))
+    return {"cases": int(len(top1)), "top1_over_best": float(top1.mean()),
+            "top1_within_5pct": float(np.mean(top1 >= 0.95)), "gated_over_best": float(gated.mean()),
+            "gated_within_5pct": float(np.mean(gated >= 0.95)), "fallback_fraction": float(np.mean(fb)),
+            "default_over_best": float(dflt.mean()), "default_within_5pct": float(np.mean(dflt >= 0.95)),
+            "gain_over_default": float(np.mean(top1 / dflt))}
+
+
+def evaluate(model: MLP, corpus: Path, log=print, threshold: float = 0.1, topk: int = 2, time_cases: int = 100,
+             fresh_cases: int = 100, fresh_reps: int = 10) -> dict:
+    """Held-out evaluation.
+
+    1. Stored measurements (every held-out problem): model top-1, model with its measured fallback,
+       and the planner default, each over the best GB/s of the exhaustive search.
+    2. Fresh head to head (first `fresh_cases` problems): the exhaustive search's winner, the
+       model's top-1 and the default are timed again, alternately, so that the search's winner
+       loses the selection bias of being the maximum of noisy timings.
+    3. Tuning time (first `time_cases` problems): the exhaustive search's recorded wall time
+       against the model's (candidate planning, features, GPU inference, and the top-k timings
+       when it falls back)."""
+    z = np.load(corpus)
+    y, case = z["y"], z["case"]
+    meta = json.loads(bytes(z["meta"]).decode())
+    X, _ = corpus_features(meta)
+    pred = model.predict(X)
+    res = {"stored": {"threshold": threshold, "topk": topk,
+                      **stored_selection(pred, y, case, meta, model.rmse, threshold, topk)},
+           "stored_curve": [dict(threshold=t, topk=kk, **{k: v for k, v in stored_selection(
+               pred, y, case, meta, model.rmse, t, kk).items() if k in ("gated_over_best", "fallback_fraction")})
+                            for t in (0.0, 0.05, 0.1, 0.2, 0.35) for kk in (2, 4)]}
+    index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
     cases = meta["cases"]
+    search_s = z["search_s"]
+
+    # fresh head to head
+    h2h = []
+    for c in cases[:fresh_cases]:
+        k = int(c["index"])
+        rows = np.nonzero(case == k)[0]
+        tunings = meta["tunings"][index_of[k]]
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        picks = [tunings[int(np.argmax(y[rows]))], tunings[int(np.argmax(pred[rows]))], {}]
+        bench = Bench(p, seed=k)
+        best_ms = [float("inf")] * 3
+        for rnd in range(2):
+            order = [0, 1, 2] if rnd == 0 else [2, 1, 0]
+            res_r = measure(p, [picks[i] for i in order], reps=fresh_reps, verify=False, bench=bench)
+            for i, r in zip(order, res_r):
+                best_ms[i] = min(best_ms[i], r.time_ms)
+        del bench
+        h2h.append([best_ms[0] / best_ms[1], best_ms[0] / best_ms[2]])
+    if h2h:
+        h = np.asarray(h2h)
+        res["fresh"] = {"cases": int(len(h)), "reps": fresh_reps, "model_over_search": float(h[:, 0].mean()),
+                        "model_within_5pct": float(np.mean(h[:, 0] >= 0.95)),
+                        "default_over_search": float(h[:, 1].mean()),
+                        "default_within_5pct": float(np.mean(h[:, 1] >= 0.95))}
+
+    # tuning time
+    t_top1, t_gated, t_search, fbs = [], [], [], 0
     for i, c in enumerate(cases[:time_cases]):
         p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        r = select(p, confidence=0.0, model=model, verify=False, measure_choice=False)
+        t_top1.append(r["seconds"])
         r = select(p, confidence=threshold, model=model, topk=topk, verify=False, measure_choice=False)
-        t_sel.append(r["seconds"])
+        t_gated.append(r["seconds"])
+        fbs += int(r["fallback"])
         t_search.append(search_s[i])
-    res = {"cases": int(len(ratios)), "model_over_best_mean": float(ratios.mean()),
-           "model_over_best_median": float(np.median(ratios)), "model_within_5pct": float(np.mean(ratios >= 0.95)),
-           "default_over_best_mean": float(default_ratios.mean()),
-           "default_within_5pct": float(np.mean(default_ratios >= 0.95)),
-           "gain_over_default_mean": float(np.mean(ratios / default_ratios)),
-           "fallback_fraction": fallbacks / max(1, len(ratios)),
-           "search_seconds_mean": float(np.mean(t_search)), "model_seconds_mean": float(np.mean(t_sel)),
-           "tuning_time_ratio": float(np.mean(t_search) / max(np.mean(t_sel), 1e-9)),
-           "threshold": threshold, "topk": topk, "rmse": model.rmse}
+    res["time"] = {"cases": len(t_search), "search_seconds_mean": float(np.mean(t_search)),
+                   "model_top1_seconds_mean": float(np.mean(t_top1)),
+                   "model_gated_seconds_mean": float(np.mean(t_gated)),
+                   "top1_speedup": float(np.mean(t_search) / max(np.mean(t_top1), 1e-9)),
+                   "gated_speedup": float(np.mean(t_search) / max(np.mean(t_gated), 1e-9)),
+                   "gated_fallbacks": fbs}
+    res["rmse"] = model.rmse
     if log:
         log(json.dumps(res, indent=1))
     return res
@@ -492,7 +567,8 @@ def main(argv=None):
     ap.add_argument("--model", default=str(DEFAULT_MODEL))
     ap.add_argument("--max-impl", type=int, default=64)
     ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--threshold", type=float, default=0.35)
+    ap.add_argument("--threshold", type=float, default=0.1)
+    ap.add_argument("--topk", type=int, default=2)
     ap.add_argument("--out-json", default=None)
     ap.add_argument("--max-seconds", type=float, default=None, help="collect: stop (resumably) after this long")
     a = ap.parse_args(argv)
@@ -504,13 +580,14 @@ def main(argv=None):
             collect(wl.learning_cases(12345, a.test_cases), test_path, a.max_impl, deadline=deadline)
     elif a.cmd == "train":
         z = np.load(train_path)
-        m = train(z["X"], z["y"], epochs=a.epochs)
+        X, case = corpus_features(json.loads(bytes(z["meta"]).decode()))
+        m = train(X, z["y"], epochs=a.epochs, groups=case)
         digest = hashlib.sha256(z["X"].tobytes()[:1 << 20]).hexdigest()[:16]
         m.save(Path(a.model), {"trained_rows": int(len(z["y"])), "corpus_digest": digest})
         print(f"saved {a.model} (val rmse {m.rmse:.4f})")
     else:
         m = MLP.load(Path(a.model))
-        res = evaluate(m, test_path, threshold=a.threshold)
+        res = evaluate(m, test_path, threshold=a.threshold, topk=a.topk)
         if a.out_json:
             Path(a.out_json).write_text(json.dumps(res, indent=1))
 

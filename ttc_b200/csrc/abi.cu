@@ -276,6 +276,7 @@ size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, con
                              int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tunings, int n, char* buf,
                              size_t len) {
   std::string js = "[";
+  plan_tile_cache_begin();
   for (int k = 0; k < n; ++k) {
     ttcb_plan p;
     p.shape_only = true;
@@ -299,6 +300,7 @@ size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, con
     js += (k ? "," : "");
     js += ok ? plan_describe_json(&p) : std::string("null");
   }
+  plan_tile_cache_end();
   js += "]";
   if (buf && len) {
     size_t m = std::min(len - 1, js.size());

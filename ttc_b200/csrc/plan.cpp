@@ -241,11 +241,14 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   // too few tiles to fill 148 SMs
   double need = 148.0 * 4;
   if ((double)ntiles < need) cost *= 1.0 + 0.5 * (need - ntiles) / need;
-  if (tu.run_bytes > 0) {
-    double r = std::log2(std::max(1.0, (double)c.LA * EA) / tu.run_bytes);
-    cost *= 1.0 + 0.25 * std::fabs(r);
-  }
   c.cost = cost;
+}
+
+// The run-length knob: a preference for A runs near tu.run_bytes, as a factor on the cost.
+static double run_bytes_factor(const TileCand& c, int EA, const ttcb_tuning& tu) {
+  if (tu.run_bytes <= 0) return 1.0;
+  const double r = std::log2(std::max(1.0, (double)c.LA * EA) / tu.run_bytes);
+  return 1.0 + 0.25 * std::fabs(r);
 }
 
 static void block_choices(int64_t n, int64_t prefix, int EA, std::vector<int64_t>& out) {
@@ -262,12 +265,20 @@ static void block_choices(int64_t n, int64_t prefix, int EA, std::vector<int64_t
   out.erase(std::unique(out.begin(), out.end()), out.end());
 }
 
-static bool best_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& best) {
+static int64_t tile_pmax(int EA, const ttcb_tuning& tu) {
+  const int64_t Pmax = tu.tile_elems > 0 ? tu.tile_elems : 16384 / EA;
+  return std::min<int64_t>(Pmax, 8192);
+}
+
+// Every admissible tile shape with at most Pmax elements, in enumeration order, evaluated without
+// the run-length knob (which only scales the cost).
+static void enumerate_tiles(const FusedProblem& f, int EA, int EB, bool beta, int vec_knob, int64_t Pmax,
+                            std::vector<TileCand>& out) {
+  out.clear();
   const int r = f.rank;
-  int64_t Pmax = tu.tile_elems > 0 ? tu.tile_elems : 16384 / EA;
-  Pmax = std::min<int64_t>(Pmax, 8192);
-  int64_t maxseg = 1024;
-  bool found = false;
+  const int64_t maxseg = 1024;
+  ttcb_tuning tu{};
+  tu.vec = vec_knob;
   std::vector<int64_t> chA, chB;
   for (int kA = 1; kA <= r; ++kA) {
     int64_t prefA = 1;
@@ -311,16 +322,77 @@ static bool best_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
           if (nblk > 2) continue;
           eval_tile(f, EA, EB, beta, tu, c);
           if (c.P / c.LA > maxseg || c.P / c.LB > maxseg) continue;
-          if (!found || c.cost < best.cost - 1e-9 ||
-              (std::fabs(c.cost - best.cost) <= 1e-9 && std::min(c.LA, c.LB) > std::min(best.LA, best.LB))) {
-            best = c;
-            found = true;
-          }
+          out.push_back(c);
         }
       }
     }
   }
+}
+
+// The cheapest enumerated tile under the tuning's size limit and run-length preference (ties go to
+// the longer shorter run).
+static bool pick_tile(const std::vector<TileCand>& cands, int EA, const ttcb_tuning& tu, TileCand& best) {
+  const int64_t Pmax = tile_pmax(EA, tu);
+  bool found = false;
+  for (const TileCand& c0 : cands) {
+    if (c0.P > Pmax) continue;
+    TileCand c = c0;
+    c.cost *= run_bytes_factor(c, EA, tu);
+    if (!found || c.cost < best.cost - 1e-9 ||
+        (std::fabs(c.cost - best.cost) <= 1e-9 && std::min(c.LA, c.LB) > std::min(best.LA, best.LB))) {
+      best = c;
+      found = true;
+    }
+  }
   return found;
+}
+
+// Planning several tunings of one problem (the learned selector's candidates) enumerates the tile
+// shapes once: while a TileEnumCache is installed on this thread, best_tile reuses its list for
+// the same fused problem, types and access-width knob.
+struct TileEnumCache {
+  bool valid = false;
+  FusedProblem f;
+  int EA = 0, EB = 0, vec = 0;
+  bool beta = false;
+  std::vector<TileCand> cands;
+};
+static thread_local TileEnumCache* g_tile_cache = nullptr;
+
+static bool same_fused(const FusedProblem& a, const FusedProblem& b) {
+  if (a.rank != b.rank) return false;
+  for (int i = 0; i < a.rank; ++i)
+    if (a.perm[i] != b.perm[i] || a.n[i] != b.n[i] || a.sA[i] != b.sA[i] || a.sB[i] != b.sB[i]) return false;
+  return true;
+}
+
+static bool best_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& best) {
+  const int vec = tu.vec == 1 ? 1 : 0;
+  if (TileEnumCache* c = g_tile_cache) {
+    if (!c->valid || c->EA != EA || c->EB != EB || c->beta != beta || c->vec != vec || !same_fused(c->f, f)) {
+      enumerate_tiles(f, EA, EB, beta, vec, 8192, c->cands);
+      c->valid = true;
+      c->f = f;
+      c->EA = EA;
+      c->EB = EB;
+      c->beta = beta;
+      c->vec = vec;
+    }
+    return pick_tile(c->cands, EA, tu, best);
+  }
+  std::vector<TileCand> cands;
+  enumerate_tiles(f, EA, EB, beta, vec, tile_pmax(EA, tu), cands);
+  return pick_tile(cands, EA, tu, best);
+}
+
+void plan_tile_cache_begin() {
+  if (!g_tile_cache) g_tile_cache = new TileEnumCache();
+  g_tile_cache->valid = false;
+}
+
+void plan_tile_cache_end() {
+  delete g_tile_cache;
+  g_tile_cache = nullptr;
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -59,6 +59,11 @@ struct ttcb_plan {
 // message in err on failure.
 ttcb_status plan_build_host(ttcb_plan* p, std::string& err);
 
+// Between these calls, plan_build_host on this thread enumerates the tile shapes of a problem once
+// and reuses them for further tunings of the same problem (used to plan many candidates quickly).
+void plan_tile_cache_begin();
+void plan_tile_cache_end();
+
 // Fusion of adjacent dimensions that stay adjacent in B (exposed for tests through the C ABI of
 // the test helper in abi.cu).
 void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA, const int64_t* sB,
