@@ -70,7 +70,7 @@ def parse_tile(b):
     L = layout()
     names = ["P", "LA", "LB", "nsegA", "nsegB", "pshift", "pad", "phys_size", "ngrid", "nblocked", "ntiles",
              "off_segA", "off_segB", "off_perm", "smem_bytes", "fast", "async_ok", "padA", "stage_elems",
-             "nstages", "off_gtab", "sigmaA"]
+             "nstages", "off_gtab", "sigmaA", "reg_ok", "rag_a", "rag_b", "nrag0", "nrag1"]
     t = {k: _i32(b, 4 * i) for i, k in enumerate(names)}
     t["divLA"] = _fd(b, L["off_divLA"])
     t["divLB"] = _fd(b, L["off_divLA"] + L["fastdiv_size"])
@@ -137,6 +137,7 @@ def simulate_tile(t):
     assert len(np.unique(t["ptab"])) == P, "two elements share a shared-memory slot"
     assert set(t["ptab"].tolist()) == set(slot_q.tolist()), "load and store slots differ"
     a_out, b_out = [], []
+    ragged = []
     for tile in range(t["ntiles"]):
         rem = tile
         bA = bB = 0
@@ -149,6 +150,8 @@ def simulate_tile(t):
             bB += blk * g["strideB"]
             if g["blocked"] >= 0:
                 lim[g["blocked"]] = min(g["e"], g["n"] - blk * g["e"])
+                if lim[g["blocked"]] < g["e"]:
+                    ragged.append(tile)
         okA = np.ones(P, bool)
         okB = np.ones(P, bool)
         for k, bd in enumerate(t["bd"]):
@@ -165,8 +168,33 @@ def simulate_tile(t):
         assert (src >= 0).all(), "store phase reads a slot the load phase did not write"
         a_out.append(src)
         b_out.append(bB + b_rel[okB])
+    # the staged kernel leaves ragged tiles to the ragged-tile kernel, which enumerates them by index
+    want = sorted(set(ragged))
+    got = [ragged_tile_index(t, r) for r in range(t["nrag0"] + t["nrag1"])]
+    assert len(got) == len(set(got)), "a ragged tile is enumerated twice"
+    assert sorted(got) == want, "ragged-tile enumeration differs from the ragged tiles"
     return np.concatenate(a_out) if a_out else np.zeros(0, np.int64), \
         np.concatenate(b_out) if b_out else np.zeros(0, np.int64)
+
+
+def ragged_tile_index(t, r):
+    """The ragged-tile kernel's r -> tile index (mixed radix with the ragged dimension pinned)."""
+    fixed, excl = t["rag_a"], -1
+    if r >= t["nrag0"]:
+        r -= t["nrag0"]
+        fixed, excl = t["rag_b"], t["rag_a"]
+    tile, M = 0, 1
+    for k, g in enumerate(t["g"]):
+        cnt = g["div"][0]
+        if k == fixed:
+            c = cnt - 1
+        else:
+            radix = cnt - 1 if k == excl else cnt
+            c = r % radix
+            r //= radix
+        tile += c * M
+        M *= cnt
+    return tile
 
 
 def simulate_row(r):

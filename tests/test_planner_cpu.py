@@ -187,3 +187,27 @@ def test_shape_only_plans_match_full_plans():
             if full["kernel"] == "tile":
                 for k in ("P", "LA", "LB", "ntiles", "ext"):
                     assert sh["tile"][k] == full["tile"][k], (perm, size, dtype, tu, k)
+
+
+def test_ragged_tile_enumeration_covers_every_ragged_tile_once():
+    """The staged kernel moves complete tiles only; the ragged-tile kernel enumerates the others by
+    index (kernel_sim.simulate_tile checks the enumeration against a scan of every tile)."""
+    rng = np.random.default_rng(2)
+    seen_two = seen_one = 0
+    for it in range(300):
+        r = int(rng.integers(2, 6))
+        size = [int(x) for x in rng.integers(2, 40, r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        for tu in (None, {"tile_elems": 256}, {"tile_elems": 64}):
+            try:
+                kind, b = kernel_sim.host_desc(perm, size, "s", False, None, None, tu)
+            except TTCError:
+                continue
+            if kind != 1:
+                continue
+            t = kernel_sim.parse_tile(b)
+            if t["nrag0"] > 0 and t["ntiles"] < 3000:
+                kernel_sim.simulate_tile(t)
+                seen_one += 1
+                seen_two += t["nrag1"] > 0
+    assert seen_one > 100 and seen_two > 5

@@ -93,7 +93,8 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     work = (rd->nunits + (ttcb::kThreads / 32) - 1) / (ttcb::kThreads / 32);  // one warp per unit
   }
-  auto grid_for = [&](int kernel_id, int smem, int* out) -> ttcb_status {
+  auto grid_for = [&](int kernel_id, int smem, int* out, int64_t items = -1) -> ttcb_status {
+    const int64_t work_k = items >= 0 ? std::max<int64_t>(items, 1) : work;
     ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel_id, p->vecA, p->vecB, variant_of(p));
     if (!k.func) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
     if (needs_large_smem(smem)) allow_large_smem(k.func);
@@ -103,11 +104,11 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
     int64_t resident = (int64_t)per_sm * sms;
     int64_t blocks;
-    if (p->tuning.blocks > 0) {
-      blocks = std::min<int64_t>(p->tuning.blocks, work);
+    if (p->tuning.blocks > 0 && items < 0) {
+      blocks = std::min<int64_t>(p->tuning.blocks, work_k);
     } else {
-      int64_t per = (work + resident - 1) / resident;  // work items per CTA, balanced
-      blocks = (work + per - 1) / per;
+      int64_t per = (work_k + resident - 1) / resident;  // work items per CTA, balanced
+      blocks = (work_k + per - 1) / per;
     }
     *out = (int)std::max<int64_t>(blocks, 1);
     return TTCB_OK;
@@ -124,6 +125,10 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       s = grid_for(td->reg_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async,
                    &p->blocks_async);
       if (s != TTCB_OK) return s;
+      if (td->nrag0 + td->nrag1 > 0) {
+        s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_bytes, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
+        if (s != TTCB_OK) return s;
+      }
     }
   }
   return TTCB_OK;
@@ -225,6 +230,17 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
   if (needs_large_smem(smem)) allow_large_smem(k.func);
   e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), blocks);
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  if (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG) {
+    // the staged kernel moves complete tiles only; the ragged ones follow on the same stream
+    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    if (td->nrag0 + td->nrag1 > 0) {
+      ttcb::KernelRef kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
+      if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
+      if (needs_large_smem(p->smem_bytes)) allow_large_smem(kr.func);
+      e = kr.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), p->blocks_ragged);
+      if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
+    }
+  }
   return TTCB_OK;
 }
 

@@ -59,7 +59,11 @@ struct TileDesc {
   int32_t off_gtab;   // byte offset of gtab (uint16_t[P]) from the start of the descriptor
   int32_t sigmaA;     // staged layout: element p at p + (p / sigmaA) * padA
   int32_t reg_ok;     // 1: fast, and the staged tile's byte offsets fit 16 bits (register path)
-  int32_t pad2_[1];
+  // ragged tiles (last block of a blocked dimension that does not divide its extent), which the
+  // staged kernel leaves to the ragged-tile kernel: grid dimensions rag_a, rag_b (-1: none);
+  // tiles with rag_a at its last block come first (nrag0), then those with rag_b at its last block
+  // and rag_a not (nrag1)
+  int32_t rag_a, rag_b, nrag0, nrag1;
   FastDiv divLA, divLB;
   FastDiv divSigmaA;
   GridDimDesc g[TTCB_MAXR];
@@ -83,4 +87,4 @@ enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };
 // launch-time variant of a tile plan (never stored in a plan's kernel field)
 // Launch-time kernel choices for tile plans: register-prefetch kernel, staged kernel with offsets
 // computed from the run tables, staged kernel with offsets held in registers.
-enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5 };
+enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5, TTCB_KERNEL_TILE_RAGGED = 6 };

@@ -152,16 +152,6 @@ __device__ __forceinline__ void tile_ragged(const TileDesc& d, const TileTables&
   __syncthreads();
 }
 
-// The ragged path as a call, for kernels whose steady state keeps many offsets in registers: the
-// registers live across it are saved only when a ragged tile actually occurs.
-template <typename TA, typename TB, bool BETA, bool STREAM>
-__device__ __noinline__ void tile_ragged_call(const TileDesc& d, TileTables tt, int lim0, int lim1,
-                                              const TA* __restrict__ At, TB* __restrict__ Bt, TA alpha, TB beta,
-                                              TA* tile) {
-  const int lim[2] = {lim0, lim1};
-  tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, At, Bt, alpha, beta, tile);
-}
-
 // One tile with the generic table-driven loops: load phase (A runs -> alpha*A -> shared slots in B
 // order), barrier, store phase (shared slots -> B runs, with beta*B when BETA), barrier.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM>
@@ -277,6 +267,66 @@ __global__ void __launch_bounds__(kThreads, 4) tile_kernel(const TileDesc* __res
   const uint32_t ntiles = (uint32_t)d.ntiles;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x)
     tile_body<TA, TB, VA, VB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
+}
+
+// Tile index of the r-th ragged tile (see TileDesc::rag_a): mixed radix over the grid dimensions
+// with the ragged dimension pinned to its last block (and, in the second part, rag_a below its last).
+__device__ __forceinline__ uint32_t ragged_tile_index(const TileDesc& d, uint32_t r) {
+  int fixed = d.rag_a, excl = -1;
+  if (r >= (uint32_t)d.nrag0) {
+    r -= (uint32_t)d.nrag0;
+    fixed = d.rag_b;
+    excl = d.rag_a;
+  }
+  uint32_t t = 0, M = 1;
+  for (int k = 0; k < d.ngrid; ++k) {
+    const uint32_t cnt = d.g[k].div.d;
+    uint32_t c;
+    if (k == fixed) {
+      c = cnt - 1;
+    } else {
+      const uint32_t radix = (k == excl) ? cnt - 1 : cnt;
+      c = r % radix;
+      r /= radix;
+    }
+    t += c * M;
+    M *= cnt;
+  }
+  return t;
+}
+
+// The ragged tiles of a plan whose complete tiles the staged kernel moved: element-wise, with the
+// generic kernel's shared-memory layout (slots, then the run tables).
+template <typename TA, typename TB, bool BETA, bool STREAM>
+__global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc* __restrict__ desc,
+                                                                  const TA* __restrict__ A, TB* __restrict__ B,
+                                                                  TA alpha, TB beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const TileDesc& d = *desc;
+  const int tid = threadIdx.x;
+  TA* tile = reinterpret_cast<TA*>(smem_raw);
+  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + tile_slots_bytes(d.phys_size, sizeof(TA)));
+  int64_t* segB = segA + d.nsegA;
+  uint16_t* ptab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+  {
+    const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
+    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
+    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
+    const uint32_t* gP = reinterpret_cast<const uint32_t*>(base + d.off_perm);
+    uint32_t* sP = reinterpret_cast<uint32_t*>(ptab);
+    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
+    for (int i = tid; i < (d.P + 1) / 2; i += kThreads) sP[i] = gP[i];
+  }
+  __syncthreads();
+  const TileTables tt{segA, segB, ptab};
+  const uint32_t R = (uint32_t)(d.nrag0 + d.nrag1);
+  for (uint32_t r = blockIdx.x; r < R; r += gridDim.x) {
+    int64_t bA, bB;
+    int lim[2];
+    decode_tile(d, ragged_tile_index(d, r), bA, bB, lim);
+    tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, A + bA, B + bB, alpha, beta, tile);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -597,7 +647,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   };
 
   auto issue = [&](const TileInfo& ti, int stage) {
-    if (ti.state != 1) return;  // ragged tiles are read by the ragged path
+    if (ti.state != 1) return;  // ragged tiles are moved by the ragged-tile kernel
     const TA* At = A + ti.bA;
     const TB* Bt = B + ti.bB;
     const uint32_t sb = stage0 + (uint32_t)stage * sbytes;
@@ -715,13 +765,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
           }
         }
       }
-    } else {
-      const TileTables tg{reinterpret_cast<const int64_t*>(base + d.off_segA),
-                          reinterpret_cast<const int64_t*>(base + d.off_segB),
-                          reinterpret_cast<const uint16_t*>(base + d.off_perm)};
-      tile_ragged_call<TA, TB, BETA, STREAM>(d, tg, ti.lim0, ti.lim1, A + ti.bA, Bt, alpha, beta,
-                                             reinterpret_cast<TA*>(smem_raw + cur * sbytes));
-    }
+    }  // ragged tiles (state 0) belong to the ragged-tile kernel launched after this one
     __syncthreads();
     cur = cur + 1 == S ? 0 : cur + 1;
   }

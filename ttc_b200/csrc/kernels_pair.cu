@@ -164,6 +164,34 @@ static KernelRef tile_ref_ab(int va, int vb, int variant) {
   return tile_ref_b<1, FAST>(vb, variant);
 }
 
+template <bool BETA, bool STREAM>
+static cudaError_t launch_ragged(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
+                                 cudaStream_t stream, int blocks) {
+  TA al;
+  std::memcpy(&al, alpha, sizeof(TA));
+  TB be;
+  std::memset(&be, 0, sizeof(TB));
+  if (BETA) std::memcpy(&be, beta, sizeof(TB));
+  tile_ragged_kernel<TA, TB, BETA, STREAM><<<blocks, kThreads, p->smem_bytes, stream>>>(
+      reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
+  return cudaGetLastError();
+}
+
+static KernelRef ragged_ref(int variant) {
+  KernelRef r;
+  if (variant == 2) {
+    r.fn = &launch_ragged<true, false>;
+    r.func = reinterpret_cast<const void*>(&tile_ragged_kernel<TA, TB, true, false>);
+  } else if (variant == 1) {
+    r.fn = &launch_ragged<false, true>;
+    r.func = reinterpret_cast<const void*>(&tile_ragged_kernel<TA, TB, false, true>);
+  } else {
+    r.fn = &launch_ragged<false, false>;
+    r.func = reinterpret_cast<const void*>(&tile_ragged_kernel<TA, TB, false, false>);
+  }
+  return r;
+}
+
 template <int V>
 static KernelRef row_ref(int variant) {
   KernelRef r;
@@ -193,6 +221,7 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
   if (kernel == TTCB_KERNEL_TILE_FAST) return tile_ref_ab<true>(va, vb, variant);
   if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false>(va, vb, variant);
   if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_RAGGED) return ragged_ref(variant);
   return tile_ref_ab<false>(va, vb, variant);
 }
 

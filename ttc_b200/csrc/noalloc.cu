@@ -126,6 +126,25 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   const int64_t per = (work + resident - 1) / resident;
   p.blocks_async = (int)std::max<int64_t>((work + per - 1) / per, 1);
   e = k.fn(&p, A, B, alpha, beta, st, p.blocks_async);
+  if (e == cudaSuccess && td->nrag0 + td->nrag1 > 0) {
+    // the staged kernel moves complete tiles only; the ragged ones follow on the same stream
+    ttcb::KernelRef kr = ttcb::pick_kernel(p.ta, p.tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant);
+    if (!kr.fn) {
+      p.dev_desc = nullptr;
+      return na_fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
+    }
+    if (p.smem_bytes > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(kr.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_bytes)) != cudaSuccess) {
+      p.dev_desc = nullptr;
+      return na_cuda(e, "cudaFuncSetAttribute");
+    }
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr.func, ttcb::kThreads, p.smem_bytes)) ==
+        cudaSuccess) {
+      const int64_t rw = (int64_t)td->nrag0 + td->nrag1, rres = (int64_t)std::max(per_sm, 1) * sms;
+      const int64_t rper = (rw + rres - 1) / rres;
+      e = kr.fn(&p, A, B, alpha, beta, st, (int)std::max<int64_t>((rw + rper - 1) / rper, 1));
+    }
+  }
   p.dev_desc = nullptr;  // the scratch belongs to the library, not to this stack plan
   if (e != cudaSuccess) return na_cuda(e, "kernel launch");
   return TTCB_OK;

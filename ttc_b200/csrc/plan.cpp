@@ -574,6 +574,19 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   td.ngrid = ng;
   td.nblocked = nb;
   td.ntiles = (int32_t)ntiles;
+  td.rag_a = td.rag_b = -1;
+  for (int k = 0; k < ng; ++k)
+    if (td.g[k].blocked >= 0 && td.g[k].n % td.g[k].e != 0) {
+      if (td.rag_a < 0)
+        td.rag_a = k;
+      else
+        td.rag_b = k;
+    }
+  {
+    const int64_t ca = td.rag_a >= 0 ? td.g[td.rag_a].div.d : 1, cb = td.rag_b >= 0 ? td.g[td.rag_b].div.d : 1;
+    td.nrag0 = td.rag_a >= 0 ? (int32_t)(ntiles / ca) : 0;
+    td.nrag1 = td.rag_b >= 0 ? (int32_t)(ntiles / ca / cb * (ca - 1)) : 0;
+  }
 
   auto al16 = [](int64_t x) { return (x + 15) & ~int64_t(15); };
   int64_t off = al16(sizeof(TileDesc));
