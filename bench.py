@@ -49,10 +49,11 @@ def parse():
     ap.add_argument("--cpu-sample-cases", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case", "configs"],
                     help="sweep: the 64-case 200 MiB sweep (default); batched: 4096 small transpositions "
                          "in one persistent launch against per-call launches; case: one sweep case run "
-                         "--reps times with its default plan (a small command for profilers)")
+                         "--reps times with its default plan (a small command for profilers); configs: the "
+                         "README shape and the strided mixed-precision shapes, each timed alone")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
     ap.add_argument("--reps", type=int, default=3, help="case: launches")
     ap.add_argument("--batch-count", type=int, default=4096)
@@ -232,6 +233,8 @@ def main():
         return run_batched(args, rank, world, local)
     if args.workload == "case":
         return run_case(args)
+    if args.workload == "configs":
+        return run_configs(args)
 
     import torch
     import torch.distributed as dist
@@ -419,6 +422,56 @@ def run_e2e(args, items, stream, dev, world):
             "d2h_bytes_per_step": d2h, "cases": len(sub), "ms_per_step": round(ms, 3),
             "note": ("pinned host A (and B when beta != 0) copied in and B copied out for every case inside the "
                      "timed region; copy-in and copy-out on separate streams (PCIe both directions)")}
+
+
+def run_configs(args):
+    """The single-problem configurations: TTC's README shape (perm 1,0,2 / 1000,768,16, fp32,
+    alpha = beta = 1) and the strided mixed-precision shape (perm 3,1,0,2 / 96,80,72,64, lda + 8,0,4,0;
+    z->c with alpha = (0.5, 0.25) and d->s with alpha = 0.5, beta = 0). Inputs uniform[-1,1] from the
+    seed (B from seed + 1), resident; the L2 is flushed (2x its size written) before every timed
+    launch; CUDA events, `--steps` launches after `--warmup`. Prints one JSON line."""
+    import torch
+    import ttc_b200.workloads as wl
+    from ttc_b200 import Plan
+    tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
+    flush = torch.empty(2 * 126 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = []
+    for name, c in [("readme_1000x768x16_s_beta1", wl.readme_case())] + \
+                   [(f"strided_96x80x72x64_{c['dtype']}", c) for c in wl.strided_cases()]:
+        ta, tb = (c["dtype"][0], c["dtype"][1]) if len(c["dtype"]) == 2 else (c["dtype"], c["dtype"])
+        lda = c.get("lda") or c["size"]
+        na = math.prod(lda[:-1]) * c["size"][-1]
+        nb = math.prod(c["size"])
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(args.seed)
+        A = (torch.rand(na, dtype=tmap[ta], device="cuda", generator=gen) * 2 - 1)
+        gen.manual_seed(args.seed + 1)
+        B = (torch.rand(nb, dtype=tmap[tb], device="cuda", generator=gen) * 2 - 1)
+        plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, lda=c.get("lda"))
+        for _ in range(args.warmup):
+            plan(A, B, c["alpha"], c["beta"])
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan(A, B, c["alpha"], c["beta"])
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        med = statistics.median(ms)
+        peak, src = measured_peak_gbs()
+        d = plan.describe()
+        out.append({"config": name, "perm": c["perm"], "size": c["size"], "lda": c.get("lda"), "dtype": c["dtype"],
+                    "alpha": str(c["alpha"]), "beta": c["beta"], "bytes": plan.bytes,
+                    "GBps_median": round(plan.bytes / (med / 1e3) / 1e9, 1),
+                    "GBps_best": round(plan.bytes / (min(ms) / 1e3) / 1e9, 1),
+                    "pct_of_hbm_peak": round(100 * plan.bytes / (med / 1e3) / 1e9 / peak, 1),
+                    "kernel": d["kernel"], "tile": d.get("tile"), "vec": [d["vecA"], d["vecB"]]})
+        plan.close()
+    print(json.dumps({"workload": "configs", "steps": args.steps, "warmup": args.warmup, "l2": "flushed",
+                      "results": out}), flush=True)
+    return 0
 
 
 def run_case(args):

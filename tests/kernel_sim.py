@@ -20,10 +20,10 @@ _layout = None
 def layout():
     global _layout
     if _layout is None:
-        a = (ctypes.c_int64 * 11)()
+        a = (ctypes.c_int64 * 12)()
         _native.lib().ttcb_test_desc_layout(a)
         keys = ["tile_size", "off_divLA", "off_g", "g_size", "off_bd", "bd_size", "row_size", "row_off_div",
-                "row_off_sA", "row_off_sB", "fastdiv_size"]
+                "row_off_sA", "row_off_sB", "fastdiv_size", "g_strideA"]
         _layout = dict(zip(keys, list(a)))
     return _layout
 
@@ -70,15 +70,16 @@ def parse_tile(b):
     L = layout()
     names = ["P", "LA", "LB", "nsegA", "nsegB", "pshift", "pad", "phys_size", "ngrid", "nblocked", "ntiles",
              "off_segA", "off_segB", "off_perm", "smem_bytes", "fast", "async_ok", "padA", "stage_elems",
-             "nstages", "off_gtab", "sigmaA", "reg_ok", "rag_a", "rag_b", "nrag0", "nrag1"]
+             "nstages", "off_gtab", "sigmaA", "reg_ok", "rag_a", "rag_b", "nrag0", "nrag1", "nfull"]
     t = {k: _i32(b, 4 * i) for i, k in enumerate(names)}
     t["divLA"] = _fd(b, L["off_divLA"])
     t["divLB"] = _fd(b, L["off_divLA"] + L["fastdiv_size"])
     g = []
     for k in range(t["ngrid"]):
         o = L["off_g"] + k * L["g_size"]
-        g.append({"div": _fd(b, o), "strideA": _i64(b, o + 16), "strideB": _i64(b, o + 24), "n": _i64(b, o + 32),
-                  "e": _i32(b, o + 40), "blocked": _i32(b, o + 44)})
+        g.append({"div": _fd(b, o), "divf": _fd(b, o + L["fastdiv_size"]), "strideA": _i64(b, o + L["g_strideA"]),
+                  "strideB": _i64(b, o + L["g_strideA"] + 8), "n": _i64(b, o + L["g_strideA"] + 16),
+                  "e": _i32(b, o + L["g_strideA"] + 24), "blocked": _i32(b, o + L["g_strideA"] + 28)})
     t["g"] = g
     bd = []
     for k in range(t["nblocked"]):
@@ -168,7 +169,18 @@ def simulate_tile(t):
         assert (src >= 0).all(), "store phase reads a slot the load phase did not write"
         a_out.append(src)
         b_out.append(bB + b_rel[okB])
-    # the staged kernel leaves ragged tiles to the ragged-tile kernel, which enumerates them by index
+    # the staged kernel walks the complete tiles, numbered over the divf counts
+    full = []
+    for tf in range(t["nfull"]):
+        rem, tile, M = tf, 0, 1
+        for g in t["g"]:
+            qq = int(fdiv(rem, g["divf"]))
+            tile += (rem - qq * g["divf"][0]) * M
+            rem = qq
+            M *= g["div"][0]
+        full.append(tile)
+    assert sorted(full) == sorted(set(range(t["ntiles"])) - set(ragged)), "complete-tile enumeration differs"
+    # the ragged tiles go to the ragged-tile kernel, which enumerates them by index
     want = sorted(set(ragged))
     got = [ragged_tile_index(t, r) for r in range(t["nrag0"] + t["nrag1"])]
     assert len(got) == len(set(got)), "a ragged tile is enumerated twice"

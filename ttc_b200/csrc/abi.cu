@@ -104,7 +104,7 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
     int64_t resident = (int64_t)per_sm * sms;
     int64_t blocks;
-    if (p->tuning.blocks > 0 && items < 0) {
+    if (p->tuning.blocks > 0 && kernel_id != TTCB_KERNEL_TILE_RAGGED) {
       blocks = std::min<int64_t>(p->tuning.blocks, work_k);
     } else {
       int64_t per = (work_k + resident - 1) / resident;  // work items per CTA, balanced
@@ -123,10 +123,10 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     }
     if (td->async_ok) {
       s = grid_for(td->reg_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async,
-                   &p->blocks_async);
+                   &p->blocks_async, td->nfull);
       if (s != TTCB_OK) return s;
       if (td->nrag0 + td->nrag1 > 0) {
-        s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_bytes, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
+        s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_ragged, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
         if (s != TTCB_OK) return s;
       }
     }
@@ -236,7 +236,7 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
     if (td->nrag0 + td->nrag1 > 0) {
       ttcb::KernelRef kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
       if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
-      if (needs_large_smem(p->smem_bytes)) allow_large_smem(kr.func);
+      if (needs_large_smem(p->smem_ragged)) allow_large_smem(kr.func);
       e = kr.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), p->blocks_ragged);
       if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
     }
@@ -407,6 +407,7 @@ void ttcb_test_desc_layout(int64_t* out) {
   out[8] = offsetof(RowDesc, sA);
   out[9] = offsetof(RowDesc, sB);
   out[10] = sizeof(FastDiv);
+  out[11] = offsetof(GridDimDesc, strideA);
 }
 
 uint32_t ttcb_test_fastdiv(uint32_t n, uint32_t d) {

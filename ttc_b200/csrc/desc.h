@@ -21,6 +21,7 @@
 
 struct GridDimDesc {
   FastDiv div;      // number of grid steps along this dimension
+  FastDiv divf;     // grid steps whose tile is complete (div, less the ragged last block if any)
   int64_t strideA;  // A element offset of one grid step (block extent * A stride)
   int64_t strideB;  // B element offset of one grid step
   int64_t n;        // full extent of the dimension
@@ -64,6 +65,8 @@ struct TileDesc {
   // tiles with rag_a at its last block come first (nrag0), then those with rag_b at its last block
   // and rag_a not (nrag1)
   int32_t rag_a, rag_b, nrag0, nrag1;
+  int32_t nfull;      // complete tiles (decoded over the divf counts of the grid dimensions)
+  int32_t pad3_;
   FastDiv divLA, divLB;
   FastDiv divSigmaA;
   GridDimDesc g[TTCB_MAXR];

@@ -55,6 +55,23 @@ __device__ __forceinline__ bool decode_tile(const TileDesc& d, uint32_t t, int64
   return full;
 }
 
+// Decodes complete-tile index t (numbered over the divf counts, which leave out the ragged last
+// blocks) into A/B base offsets.
+__device__ __forceinline__ void decode_full_tile(const TileDesc& d, uint32_t t, int64_t& bA, int64_t& bB) {
+  bA = 0;
+  bB = 0;
+  const int ng = d.ngrid;
+#pragma unroll 1  // a rolled loop keeps the callers' register budget
+  for (int g = 0; g < ng; ++g) {
+    const GridDimDesc& gd = d.g[g];
+    const uint32_t q = fdiv(t, gd.divf);
+    const uint32_t blk = t - q * gd.divf.d;
+    t = q;
+    bA += (int64_t)blk * gd.strideA;
+    bB += (int64_t)blk * gd.strideB;
+  }
+}
+
 struct TileTables {
   const int64_t* segA;
   const int64_t* segB;
@@ -267,66 +284,6 @@ __global__ void __launch_bounds__(kThreads, 4) tile_kernel(const TileDesc* __res
   const uint32_t ntiles = (uint32_t)d.ntiles;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x)
     tile_body<TA, TB, VA, VB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-}
-
-// Tile index of the r-th ragged tile (see TileDesc::rag_a): mixed radix over the grid dimensions
-// with the ragged dimension pinned to its last block (and, in the second part, rag_a below its last).
-__device__ __forceinline__ uint32_t ragged_tile_index(const TileDesc& d, uint32_t r) {
-  int fixed = d.rag_a, excl = -1;
-  if (r >= (uint32_t)d.nrag0) {
-    r -= (uint32_t)d.nrag0;
-    fixed = d.rag_b;
-    excl = d.rag_a;
-  }
-  uint32_t t = 0, M = 1;
-  for (int k = 0; k < d.ngrid; ++k) {
-    const uint32_t cnt = d.g[k].div.d;
-    uint32_t c;
-    if (k == fixed) {
-      c = cnt - 1;
-    } else {
-      const uint32_t radix = (k == excl) ? cnt - 1 : cnt;
-      c = r % radix;
-      r /= radix;
-    }
-    t += c * M;
-    M *= cnt;
-  }
-  return t;
-}
-
-// The ragged tiles of a plan whose complete tiles the staged kernel moved: element-wise, with the
-// generic kernel's shared-memory layout (slots, then the run tables).
-template <typename TA, typename TB, bool BETA, bool STREAM>
-__global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc* __restrict__ desc,
-                                                                  const TA* __restrict__ A, TB* __restrict__ B,
-                                                                  TA alpha, TB beta) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const TileDesc& d = *desc;
-  const int tid = threadIdx.x;
-  TA* tile = reinterpret_cast<TA*>(smem_raw);
-  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + tile_slots_bytes(d.phys_size, sizeof(TA)));
-  int64_t* segB = segA + d.nsegA;
-  uint16_t* ptab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
-  {
-    const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
-    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
-    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
-    const uint32_t* gP = reinterpret_cast<const uint32_t*>(base + d.off_perm);
-    uint32_t* sP = reinterpret_cast<uint32_t*>(ptab);
-    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
-    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
-    for (int i = tid; i < (d.P + 1) / 2; i += kThreads) sP[i] = gP[i];
-  }
-  __syncthreads();
-  const TileTables tt{segA, segB, ptab};
-  const uint32_t R = (uint32_t)(d.nrag0 + d.nrag1);
-  for (uint32_t r = blockIdx.x; r < R; r += gridDim.x) {
-    int64_t bA, bB;
-    int lim[2];
-    decode_tile(d, ragged_tile_index(d, r), bA, bB, lim);
-    tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, A + bA, B + bB, alpha, beta, tile);
-  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -628,7 +585,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     }
   }
 
-  const uint32_t ntiles = (uint32_t)d.ntiles;
+  const uint32_t ntiles = (uint32_t)d.nfull;  // the ragged tiles are the ragged-tile kernel's
   const uint32_t G = gridDim.x;
   const uint32_t stage0 = smem_u32(smem_raw);
 
@@ -637,13 +594,8 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       ti.state = -1;
       return;
     }
-    int64_t bA, bB;
-    int lim[2];
-    ti.state = decode_tile(d, t, bA, bB, lim) ? 1 : 0;
-    ti.bA = bA;
-    ti.bB = bB;
-    ti.lim0 = lim[0];
-    ti.lim1 = lim[1];
+    decode_full_tile(d, t, ti.bA, ti.bB);
+    ti.state = 1;
   };
 
   auto issue = [&](const TileInfo& ti, int stage) {
@@ -765,11 +717,172 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
           }
         }
       }
-    }  // ragged tiles (state 0) belong to the ragged-tile kernel launched after this one
+    }
     __syncthreads();
     cur = cur + 1 == S ? 0 : cur + 1;
   }
   cp_async_wait<0>();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Ragged tiles of a plan whose complete tiles the staged kernel moved. Each thread issues an
+// element-wise asynchronous copy for every valid A element of the tile straight into its B-order
+// shared-memory slot, so a whole tile of loads is in flight at once; the next ragged tile is
+// fetched into the second buffer while the current one is written out (alpha is applied on the way
+// out, which gives the same rounding as applying it on the way in).
+template <typename TA>
+__device__ __forceinline__ void ragged_issue(const TileDesc& d, const TileTables& tt, int lim0, int lim1,
+                                             const TA* __restrict__ At, TA* tile) {
+  const int P = d.P, LA = d.LA, nb = d.nblocked;
+  for (int p = threadIdx.x; p < P; p += kThreads) {
+    bool ok = true;
+    for (int b = 0; b < nb; ++b) {
+      const uint32_t c = fdiv((uint32_t)p, d.bd[b].tsA);
+      const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
+      ok = ok && ((int)cc < (b == 0 ? lim0 : lim1));
+    }
+    if (ok) {
+      const int s = (int)fdiv((uint32_t)p, d.divLA);
+      cp_async<sizeof(TA)>(smem_u32(tile + tt.ptab[p]), At + (tt.segA[s] + (p - s * LA)));
+    }
+  }
+}
+
+template <typename TA, typename TB, bool BETA, bool STREAM>
+__device__ __forceinline__ void ragged_store(const TileDesc& d, const TileTables& tt, int lim0, int lim1,
+                                             TB* __restrict__ Bt, TA alpha, TB beta, const TA* tile) {
+  const int P = d.P, LB = d.LB, nb = d.nblocked, pshift = d.pshift, pad = d.pad;
+  for (int q0 = threadIdx.x; q0 < P; q0 += kThreads * kUnroll) {
+    TB* dst[kUnroll];
+    TB bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int q = q0 + u * kThreads;
+      dst[u] = nullptr;
+      if (q < P) {
+        bool ok = true;
+        for (int b = 0; b < nb; ++b) {
+          const uint32_t c = fdiv((uint32_t)q, d.bd[b].tsB);
+          const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
+          ok = ok && ((int)cc < (b == 0 ? lim0 : lim1));
+        }
+        if (ok) {
+          const int s = (int)fdiv((uint32_t)q, d.divLB);
+          dst[u] = Bt + (tt.segB[s] + (q - s * LB));
+          if (BETA) bv[u] = ld_scalar<TB>(dst[u]);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (dst[u]) {
+        const int q = q0 + u * kThreads;
+        const TA tq = scale_a(alpha, tile[slot_of(q, pshift, pad)]);
+        TB r;
+        if (BETA)
+          r = combine<TA, TB>(tq, bv[u], beta);
+        else
+          r = finish<TA, TB>(tq);
+        st_scalar<TB>(dst[u], r, STREAM);
+      }
+    }
+  }
+}
+
+// Shared memory: two tile buffers of `slots` bytes each, then the run tables.
+__host__ __device__ inline size_t ragged_smem_bytes(int phys_size, int elem_bytes, int nsegA, int nsegB, int P) {
+  return 2 * tile_slots_bytes(phys_size, elem_bytes) + 8 * (size_t)(nsegA + nsegB) + al16((size_t)2 * P);
+}
+
+// Tile index of the r-th ragged tile (see TileDesc::rag_a): mixed radix over the grid dimensions
+// with the ragged dimension pinned to its last block (and, in the second part, rag_a below its last).
+__device__ __forceinline__ uint32_t ragged_tile_index(const TileDesc& d, uint32_t r) {
+  int fixed = d.rag_a, excl = -1;
+  if (r >= (uint32_t)d.nrag0) {
+    r -= (uint32_t)d.nrag0;
+    fixed = d.rag_b;
+    excl = d.rag_a;
+  }
+  uint32_t t = 0, M = 1;
+  for (int k = 0; k < d.ngrid; ++k) {
+    const uint32_t cnt = d.g[k].div.d;
+    uint32_t c;
+    if (k == fixed) {
+      c = cnt - 1;
+    } else {
+      const uint32_t radix = (k == excl) ? cnt - 1 : cnt;
+      c = r % radix;
+      r /= radix;
+    }
+    t += c * M;
+    M *= cnt;
+  }
+  return t;
+}
+
+template <typename TA, typename TB, bool BETA, bool STREAM>
+__global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc* __restrict__ desc,
+                                                                  const TA* __restrict__ A, TB* __restrict__ B,
+                                                                  TA alpha, TB beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ TileDesc d;
+  __shared__ TileInfo ri[2];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
+    reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
+  __syncthreads();
+  const size_t slots = tile_slots_bytes(d.phys_size, sizeof(TA));
+  auto buf = [&](int i) { return reinterpret_cast<TA*>(smem_raw + (i & 1) * slots); };
+  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + 2 * slots);
+  int64_t* segB = segA + d.nsegA;
+  uint16_t* ptab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+  {
+    const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
+    const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
+    const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
+    const uint32_t* gP = reinterpret_cast<const uint32_t*>(base + d.off_perm);
+    uint32_t* sP = reinterpret_cast<uint32_t*>(ptab);
+    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
+    for (int i = tid; i < (d.P + 1) / 2; i += kThreads) sP[i] = gP[i];
+  }
+  __syncthreads();
+  const TileTables tt{segA, segB, ptab};
+  const uint32_t R = (uint32_t)(d.nrag0 + d.nrag1);
+  uint32_t r = blockIdx.x;
+  if (r >= R) return;
+  // thread 0 locates and decodes each ragged tile (the mixed-radix index uses integer division)
+  // one iteration ahead; entry k & 1 holds the tile of iteration k
+  auto locate = [&](uint32_t rr, TileInfo& ti) {
+    int lim[2];
+    decode_tile(d, ragged_tile_index(d, rr), ti.bA, ti.bB, lim);
+    ti.lim0 = lim[0];
+    ti.lim1 = lim[1];
+  };
+  if (tid == 0) locate(r, ri[0]);
+  __syncthreads();
+  ragged_issue<TA>(d, tt, ri[0].lim0, ri[0].lim1, A + ri[0].bA, buf(0));
+  cp_async_commit();
+  for (int k = 0;; ++k) {
+    const uint32_t rn = r + gridDim.x;
+    const bool more = rn < R;
+    if (more && tid == 0) locate(rn, ri[(k + 1) & 1]);
+    __syncthreads();
+    if (more) {
+      const TileInfo& nx = ri[(k + 1) & 1];
+      ragged_issue<TA>(d, tt, nx.lim0, nx.lim1, A + nx.bA, buf(k + 1));
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const TileInfo& cu = ri[k & 1];
+    ragged_store<TA, TB, BETA, STREAM>(d, tt, cu.lim0, cu.lim1, B + cu.bB, alpha, beta, buf(k));
+    __syncthreads();
+    if (!more) break;
+    r = rn;
+  }
 }
 
 // One row-copy work unit (row, chunk) processed by one warp.

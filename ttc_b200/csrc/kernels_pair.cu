@@ -172,7 +172,7 @@ static cudaError_t launch_ragged(const ttcb_plan* p, const void* A, void* B, con
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
-  tile_ragged_kernel<TA, TB, BETA, STREAM><<<blocks, kThreads, p->smem_bytes, stream>>>(
+  tile_ragged_kernel<TA, TB, BETA, STREAM><<<blocks, kThreads, p->smem_ragged, stream>>>(
       reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
   return cudaGetLastError();
 }

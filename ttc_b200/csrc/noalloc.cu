@@ -122,7 +122,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
       cudaSuccess)
     return na_cuda(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   if (per_sm < 1) return na_fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
-  const int64_t work = td->ntiles, resident = (int64_t)per_sm * sms;
+  const int64_t work = td->nfull, resident = (int64_t)per_sm * sms;
   const int64_t per = (work + resident - 1) / resident;
   p.blocks_async = (int)std::max<int64_t>((work + per - 1) / per, 1);
   e = k.fn(&p, A, B, alpha, beta, st, p.blocks_async);
@@ -133,12 +133,13 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
       p.dev_desc = nullptr;
       return na_fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
     }
-    if (p.smem_bytes > 48 * 1024 &&
-        (e = cudaFuncSetAttribute(kr.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_bytes)) != cudaSuccess) {
+    if (p.smem_ragged + (int)ttcb::kAsyncStaticSmem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(kr.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_ragged)) !=
+            cudaSuccess) {
       p.dev_desc = nullptr;
       return na_cuda(e, "cudaFuncSetAttribute");
     }
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr.func, ttcb::kThreads, p.smem_bytes)) ==
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr.func, ttcb::kThreads, p.smem_ragged)) ==
         cudaSuccess) {
       const int64_t rw = (int64_t)td->nrag0 + td->nrag1, rres = (int64_t)std::max(per_sm, 1) * sms;
       const int64_t rper = (rw + rres - 1) / rres;

@@ -557,6 +557,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     int64_t cnt = (f.n[d] + e - 1) / e;
     GridDimDesc& g = td.g[ng++];
     g.div = make_fastdiv((uint32_t)cnt);
+    g.divf = make_fastdiv((uint32_t)(c.ext[d] > 0 && f.n[d] % e != 0 ? cnt - 1 : cnt));
     g.strideA = e * f.sA[d];
     g.strideB = e * f.sB[d];
     g.n = f.n[d];
@@ -586,6 +587,9 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     const int64_t ca = td.rag_a >= 0 ? td.g[td.rag_a].div.d : 1, cb = td.rag_b >= 0 ? td.g[td.rag_b].div.d : 1;
     td.nrag0 = td.rag_a >= 0 ? (int32_t)(ntiles / ca) : 0;
     td.nrag1 = td.rag_b >= 0 ? (int32_t)(ntiles / ca / cb * (ca - 1)) : 0;
+    int64_t nfull = 1;
+    for (int k = 0; k < ng; ++k) nfull *= td.g[k].divf.d;
+    td.nfull = (int32_t)nfull;
   }
 
   auto al16 = [](int64_t x) { return (x + 15) & ~int64_t(15); };
@@ -631,6 +635,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   std::memcpy(p->host_desc.data() + td.off_gtab, gtab.data(), 2 * P);
   p->smem_bytes = (int)smem;
   p->smem_fast = (int)al16(phys_size * EA);
+  p->smem_ragged = (int)ttcb::ragged_smem_bytes((int)phys_size, EA, (int)nsegA, (int)nsegB, (int)P);
   p->vecA = c.vecA;
   p->vecB = c.vecB;
   p->est_cost = c.cost;

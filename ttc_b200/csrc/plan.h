@@ -47,6 +47,7 @@ struct ttcb_plan {
   int smem_async = 0;     // staged tile kernel (stages + tables)
   int blocks_async = 0;   // CTAs for the staged tile kernel
   int blocks_ragged = 0;  // CTAs for the ragged-tile kernel that follows the staged kernel
+  int smem_ragged = 0;    // its dynamic shared memory (two tile buffers + tables)
   int device = 0;
 
   // shape-only planning (candidate features for the learned selector): the tile choice without
