@@ -142,6 +142,12 @@ static int64_t run_len(const std::vector<int>& order, const int64_t* ext, const 
   return L;
 }
 
+// Cost of a ragged tile relative to a complete one (per tile slot): the ragged-tile kernel checks
+// every element's coordinates and moves scalars.
+#ifndef TTCB_RAGGED_COST
+#define TTCB_RAGGED_COST 1.5
+#endif
+
 static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& c) {
   std::vector<int> aord, bord;
   tile_orders(f, c.ext, aord, bord);
@@ -230,7 +236,7 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
         int64_t nb = (f.n[d] + c.ext[d] - 1) / c.ext[d];
         full_frac *= (double)(nb - 1) / (double)nb;
       }
-    cost += (1.0 - full_frac) * per_elem * 1.5;
+    cost += (1.0 - full_frac) * per_elem * TTCB_RAGGED_COST;
   }
 
   // shared memory footprint and residency
@@ -251,12 +257,28 @@ static double run_bytes_factor(const TileCand& c, int EA, const ttcb_tuning& tu)
   return 1.0 + 0.25 * std::fabs(r);
 }
 
-static void block_choices(int64_t n, int64_t prefix, int EA, std::vector<int64_t>& out) {
+// Divisors of n in [8, 1024] (block sizes that leave no ragged last block), at most six of them
+// spread evenly over that range on a log scale.
+static void exact_blocks(int64_t n, std::vector<int64_t>& out) {
+  std::vector<int64_t> all;
+  for (int64_t b = 8; b <= 1024 && b < n; ++b)
+    if (n % b == 0) all.push_back(b);
+  out.clear();
+  if (all.size() <= 6) {
+    out = all;
+    return;
+  }
+  for (int k = 0; k < 6; ++k) out.push_back(all[(all.size() - 1) * k / 5]);
+}
+
+static void block_choices(int64_t n, int64_t prefix, int EA, const std::vector<int64_t>& exact,
+                          std::vector<int64_t>& out) {
   out.clear();
   out.push_back(n);
   static const int64_t base[] = {2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 24, 32, 48, 64, 96, 128, 192, 256, 512};
   for (int64_t b : base)
     if (b < n) out.push_back(b);
+  for (int64_t b : exact) out.push_back(b);
   for (int64_t bytes : {128, 256, 512, 1024}) {
     int64_t b = (bytes / EA + prefix - 1) / std::max<int64_t>(prefix, 1);
     if (b >= 2 && b < n) out.push_back(b);
@@ -280,17 +302,19 @@ static void enumerate_tiles(const FusedProblem& f, int EA, int EB, bool beta, in
   ttcb_tuning tu{};
   tu.vec = vec_knob;
   std::vector<int64_t> chA, chB;
+  std::vector<std::vector<int64_t>> exact(r);
+  for (int i = 0; i < r; ++i) exact_blocks(f.n[i], exact[i]);
   for (int kA = 1; kA <= r; ++kA) {
     int64_t prefA = 1;
     for (int i = 0; i < kA - 1; ++i) prefA *= f.n[i];
     if (prefA > Pmax) break;
-    block_choices(f.n[kA - 1], prefA, EA, chA);
+    block_choices(f.n[kA - 1], prefA, EA, exact[kA - 1], chA);
     for (int64_t eA : chA) {
       for (int kB = 1; kB <= r; ++kB) {
         int64_t prefB = 1;
         for (int j = 0; j < kB - 1; ++j) prefB *= f.n[f.perm[j]];
         if (prefB > Pmax) break;
-        block_choices(f.n[f.perm[kB - 1]], prefB, EB, chB);
+        block_choices(f.n[f.perm[kB - 1]], prefB, EB, exact[f.perm[kB - 1]], chB);
         for (int64_t eB : chB) {
           TileCand c;
           for (int i = 0; i < TTCB_MAXR; ++i) c.ext[i] = 0;
