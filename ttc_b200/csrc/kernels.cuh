@@ -725,33 +725,37 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
 }
 
 // ------------------------------------------------------------------------------------------------
-// Ragged tiles of a plan whose complete tiles the staged kernel moved. Each thread issues an
-// element-wise asynchronous copy for every valid A element of the tile straight into its B-order
-// shared-memory slot, so a whole tile of loads is in flight at once; the next ragged tile is
-// fetched into the second buffer while the current one is written out (alpha is applied on the way
-// out, which gives the same rounding as applying it on the way in).
+// Ragged tiles of a plan whose complete tiles the staged kernel moved. Every CTA first tabulates,
+// for each tile element, its tile-relative A and B offsets (32-bit) and its coordinates in the
+// blocked dimensions (two 16-bit fields), which do not depend on the tile; a ragged tile then costs
+// a compare per element. Each thread issues an element-wise asynchronous copy for every valid A
+// element straight into its B-order shared-memory slot, so a whole tile of loads is in flight at
+// once, and the next ragged tile is fetched into the second buffer while the current one is written
+// out (alpha is applied on the way out, which rounds exactly as applying it on the way in).
+struct RaggedTables {
+  const int32_t* relA;  // A-order element p: offset from the tile's A base
+  const uint32_t* crdA; // A-order element p: blocked coordinates (low 16 bits: dim 0, high: dim 1)
+  const int32_t* relB;  // B-order element q: offset from the tile's B base
+  const uint32_t* crdB; // B-order element q: blocked coordinates
+  const uint16_t* ptab; // A-order element p: shared-memory slot
+};
+
+__device__ __forceinline__ bool ragged_valid(uint32_t crd, int lim0, int lim1) {
+  return (int)(crd & 0xffffu) < lim0 && (int)(crd >> 16) < lim1;
+}
+
 template <typename TA>
-__device__ __forceinline__ void ragged_issue(const TileDesc& d, const TileTables& tt, int lim0, int lim1,
+__device__ __forceinline__ void ragged_issue(const TileDesc& d, const RaggedTables& rt, int lim0, int lim1,
                                              const TA* __restrict__ At, TA* tile) {
-  const int P = d.P, LA = d.LA, nb = d.nblocked;
-  for (int p = threadIdx.x; p < P; p += kThreads) {
-    bool ok = true;
-    for (int b = 0; b < nb; ++b) {
-      const uint32_t c = fdiv((uint32_t)p, d.bd[b].tsA);
-      const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-      ok = ok && ((int)cc < (b == 0 ? lim0 : lim1));
-    }
-    if (ok) {
-      const int s = (int)fdiv((uint32_t)p, d.divLA);
-      cp_async<sizeof(TA)>(smem_u32(tile + tt.ptab[p]), At + (tt.segA[s] + (p - s * LA)));
-    }
-  }
+  const int P = d.P;
+  for (int p = threadIdx.x; p < P; p += kThreads)
+    if (ragged_valid(rt.crdA[p], lim0, lim1)) cp_async<sizeof(TA)>(smem_u32(tile + rt.ptab[p]), At + rt.relA[p]);
 }
 
 template <typename TA, typename TB, bool BETA, bool STREAM>
-__device__ __forceinline__ void ragged_store(const TileDesc& d, const TileTables& tt, int lim0, int lim1,
+__device__ __forceinline__ void ragged_store(const TileDesc& d, const RaggedTables& rt, int lim0, int lim1,
                                              TB* __restrict__ Bt, TA alpha, TB beta, const TA* tile) {
-  const int P = d.P, LB = d.LB, nb = d.nblocked, pshift = d.pshift, pad = d.pad;
+  const int P = d.P, pshift = d.pshift, pad = d.pad;
   for (int q0 = threadIdx.x; q0 < P; q0 += kThreads * kUnroll) {
     TB* dst[kUnroll];
     TB bv[kUnroll];
@@ -759,18 +763,9 @@ __device__ __forceinline__ void ragged_store(const TileDesc& d, const TileTables
     for (int u = 0; u < kUnroll; ++u) {
       const int q = q0 + u * kThreads;
       dst[u] = nullptr;
-      if (q < P) {
-        bool ok = true;
-        for (int b = 0; b < nb; ++b) {
-          const uint32_t c = fdiv((uint32_t)q, d.bd[b].tsB);
-          const uint32_t cc = c - fdiv(c, d.bd[b].ext) * d.bd[b].ext.d;
-          ok = ok && ((int)cc < (b == 0 ? lim0 : lim1));
-        }
-        if (ok) {
-          const int s = (int)fdiv((uint32_t)q, d.divLB);
-          dst[u] = Bt + (tt.segB[s] + (q - s * LB));
-          if (BETA) bv[u] = ld_scalar<TB>(dst[u]);
-        }
+      if (q < P && ragged_valid(rt.crdB[q], lim0, lim1)) {
+        dst[u] = Bt + rt.relB[q];
+        if (BETA) bv[u] = ld_scalar<TB>(dst[u]);
       }
     }
 #pragma unroll
@@ -789,9 +784,9 @@ __device__ __forceinline__ void ragged_store(const TileDesc& d, const TileTables
   }
 }
 
-// Shared memory: two tile buffers of `slots` bytes each, then the run tables.
-__host__ __device__ inline size_t ragged_smem_bytes(int phys_size, int elem_bytes, int nsegA, int nsegB, int P) {
-  return 2 * tile_slots_bytes(phys_size, elem_bytes) + 8 * (size_t)(nsegA + nsegB) + al16((size_t)2 * P);
+// Shared memory: two tile buffers of `slots` bytes each, then the per-element tables.
+__host__ __device__ inline size_t ragged_smem_bytes(int phys_size, int elem_bytes, int P) {
+  return 2 * tile_slots_bytes(phys_size, elem_bytes) + 16 * (size_t)P + al16((size_t)2 * P);
 }
 
 // Tile index of the r-th ragged tile (see TileDesc::rag_a): mixed radix over the grid dimensions
@@ -831,26 +826,41 @@ __global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
     reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
   __syncthreads();
+  const uint32_t R = (uint32_t)(d.nrag0 + d.nrag1);
+  uint32_t r = blockIdx.x;
+  if (r >= R) return;
+  const int P = d.P;
   const size_t slots = tile_slots_bytes(d.phys_size, sizeof(TA));
   auto buf = [&](int i) { return reinterpret_cast<TA*>(smem_raw + (i & 1) * slots); };
-  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + 2 * slots);
-  int64_t* segB = segA + d.nsegA;
-  uint16_t* ptab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+  int32_t* relA = reinterpret_cast<int32_t*>(smem_raw + 2 * slots);
+  uint32_t* crdA = reinterpret_cast<uint32_t*>(relA + P);
+  int32_t* relB = reinterpret_cast<int32_t*>(crdA + P);
+  uint32_t* crdB = reinterpret_cast<uint32_t*>(relB + P);
+  uint16_t* ptab = reinterpret_cast<uint16_t*>(crdB + P);
   {
     const unsigned char* base = reinterpret_cast<const unsigned char*>(desc);
     const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
     const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
-    const uint32_t* gP = reinterpret_cast<const uint32_t*>(base + d.off_perm);
-    uint32_t* sP = reinterpret_cast<uint32_t*>(ptab);
-    for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
-    for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
-    for (int i = tid; i < (d.P + 1) / 2; i += kThreads) sP[i] = gP[i];
+    const uint16_t* gP = reinterpret_cast<const uint16_t*>(base + d.off_perm);
+    const int nb = d.nblocked;
+    for (int p = tid; p < P; p += kThreads) {
+      const int sa = (int)fdiv((uint32_t)p, d.divLA);
+      relA[p] = (int32_t)(gA[sa] + (p - sa * d.LA));
+      const int sb = (int)fdiv((uint32_t)p, d.divLB);
+      relB[p] = (int32_t)(gB[sb] + (p - sb * d.LB));
+      uint32_t ca = 0, cb = 0;
+      for (int b = 0; b < nb; ++b) {
+        const uint32_t x = fdiv((uint32_t)p, d.bd[b].tsA);
+        const uint32_t y = fdiv((uint32_t)p, d.bd[b].tsB);
+        ca |= (x - fdiv(x, d.bd[b].ext) * d.bd[b].ext.d) << (16 * b);
+        cb |= (y - fdiv(y, d.bd[b].ext) * d.bd[b].ext.d) << (16 * b);
+      }
+      crdA[p] = ca;
+      crdB[p] = cb;
+      ptab[p] = gP[p];
+    }
   }
-  __syncthreads();
-  const TileTables tt{segA, segB, ptab};
-  const uint32_t R = (uint32_t)(d.nrag0 + d.nrag1);
-  uint32_t r = blockIdx.x;
-  if (r >= R) return;
+  const RaggedTables rt{relA, crdA, relB, crdB, ptab};
   // thread 0 locates and decodes each ragged tile (the mixed-radix index uses integer division)
   // one iteration ahead; entry k & 1 holds the tile of iteration k
   auto locate = [&](uint32_t rr, TileInfo& ti) {
@@ -861,7 +871,7 @@ __global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc
   };
   if (tid == 0) locate(r, ri[0]);
   __syncthreads();
-  ragged_issue<TA>(d, tt, ri[0].lim0, ri[0].lim1, A + ri[0].bA, buf(0));
+  ragged_issue<TA>(d, rt, ri[0].lim0, ri[0].lim1, A + ri[0].bA, buf(0));
   cp_async_commit();
   for (int k = 0;; ++k) {
     const uint32_t rn = r + gridDim.x;
@@ -870,7 +880,7 @@ __global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc
     __syncthreads();
     if (more) {
       const TileInfo& nx = ri[(k + 1) & 1];
-      ragged_issue<TA>(d, tt, nx.lim0, nx.lim1, A + nx.bA, buf(k + 1));
+      ragged_issue<TA>(d, rt, nx.lim0, nx.lim1, A + nx.bA, buf(k + 1));
       cp_async_commit();
       cp_async_wait<1>();
     } else {
@@ -878,7 +888,7 @@ __global__ void __launch_bounds__(kThreads, 4) tile_ragged_kernel(const TileDesc
     }
     __syncthreads();
     const TileInfo& cu = ri[k & 1];
-    ragged_store<TA, TB, BETA, STREAM>(d, tt, cu.lim0, cu.lim1, B + cu.bB, alpha, beta, buf(k));
+    ragged_store<TA, TB, BETA, STREAM>(d, rt, cu.lim0, cu.lim1, B + cu.bB, alpha, beta, buf(k));
     __syncthreads();
     if (!more) break;
     r = rn;

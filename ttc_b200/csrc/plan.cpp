@@ -649,6 +649,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
     td.reg_ok = (td.fast && td.stage_elems * (int64_t)EA < 65536 && P * (int64_t)EB < 65536) ? 1 : 0;
+    // the staged kernel leaves ragged tiles to the ragged-tile kernel, whose tables must fit too
+    if (td.nrag0 + td.nrag1 > 0 && ttcb::ragged_smem_bytes((int)phys_size, EA, (int)P) > 200 * 1024) td.async_ok = 0;
   }
 
   p->host_desc.assign(off, 0);
@@ -659,7 +661,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   std::memcpy(p->host_desc.data() + td.off_gtab, gtab.data(), 2 * P);
   p->smem_bytes = (int)smem;
   p->smem_fast = (int)al16(phys_size * EA);
-  p->smem_ragged = (int)ttcb::ragged_smem_bytes((int)phys_size, EA, (int)nsegA, (int)nsegB, (int)P);
+  p->smem_ragged = (int)ttcb::ragged_smem_bytes((int)phys_size, EA, (int)P);
   p->vecA = c.vecA;
   p->vecB = c.vecB;
   p->est_cost = c.cost;
