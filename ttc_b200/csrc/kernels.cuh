@@ -494,14 +494,15 @@ struct TileInfo {
 
 // Static shared memory of the staged kernel (descriptor header + tile ring), on top of its dynamic
 // shared memory.
-constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + 4 * sizeof(TileInfo);
+constexpr int kInfoRing = 8;  // staged kernel: decoded-tile ring entries (tile j in entry j % 8)
+constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileInfo);
 
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
 // vectors per thread and side whose offsets fit 32 bits and whose staged bytes fit 16 bits): A
 // source offsets rA, staged byte offsets dA (two per register), B offsets rB, gather byte offsets
 // gp (two per register; B vector u = tid + u * kThreads, element j). Otherwise offsets are computed
 // per vector from the run tables in shared memory, with the gather positions in registers while
-// P <= kRegPos * kThreads and in shared memory beyond. The pipeline depth (2 or 3 stages) is the
+// P <= kRegPos * kThreads and in shared memory beyond. The number of stages (3 or 4) is the
 // descriptor's.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG>
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
-  __shared__ TileInfo info[4];  // kAsyncStaticSmem counts both
+  __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both
   const int tid = threadIdx.x;
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
     reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
@@ -653,26 +654,32 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     }
   };
 
+  // Pipeline: S stages, D = S - 2 tiles of copies in flight ahead of the tile being written, and one
+  // CTA barrier per tile. Iteration k issues tile k + D into stage (k + D) % S, whose previous tile
+  // (k - 2) every thread finished writing out before the barrier of iteration k - 1; thread 0
+  // decodes tile k + D + 2, which iteration k + 2 issues after the barrier of iteration k + 1.
+  const int D = S - 2;
   if (tid == 0)
-    for (int j = 0; j < S; ++j) decode_into(blockIdx.x + j * G, info[j]);
+    for (int j = 0; j < D + 2; ++j) decode_into(blockIdx.x + j * G, info[j]);
   __syncthreads();
-  for (int j = 0; j < S - 1; ++j) {
+  for (int j = 0; j < D; ++j) {
     issue(info[j], j);
     cp_async_commit();
   }
-  int cur = 0;  // ring slot of tile k; the slot S - 1 ahead is the one before it
+  int cur = 0;   // stage of tile k
+  int nxt = D;   // stage of tile k + D
   for (uint32_t k = 0;; ++k) {
     const uint32_t t = blockIdx.x + k * G;
     if (t >= ntiles) break;
-    issue(info[(k + S - 1) & 3], cur == 0 ? S - 1 : cur - 1);
+    issue(info[(k + D) % kInfoRing], nxt);
     cp_async_commit();
-    if (S == 3)
+    if (D == 2)
       cp_async_wait<2>();
     else
       cp_async_wait<1>();
     __syncthreads();
-    if (tid == 0) decode_into(t + S * G, info[(k + S) & 3]);
-    const TileInfo& ti = info[k & 3];
+    if (tid == 0) decode_into(t + (D + 2) * G, info[(k + D + 2) % kInfoRing]);
+    const TileInfo& ti = info[k % kInfoRing];
     TB* Bt = B + ti.bB;
     const unsigned char* stage = smem_raw + cur * sbytes;
     const TB* sB = reinterpret_cast<const TB*>(stage + a_bytes);
@@ -718,8 +725,8 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
         }
       }
     }
-    __syncthreads();
     cur = cur + 1 == S ? 0 : cur + 1;
+    nxt = nxt + 1 == S ? 0 : nxt + 1;
   }
   cp_async_wait<0>();
 }

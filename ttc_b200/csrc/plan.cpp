@@ -643,8 +643,9 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     auto smem_for = [&](int S) {
       return (int64_t)ttcb::async_smem_bytes(S, td.stage_elems, (int)P, (int)nsegA, (int)nsegB, EA, EB, beta);
     };
-    // three stages while four CTAs still fit an SM (about 56 KB each), else two
-    td.nstages = smem_for(3) <= 56 * 1024 ? 3 : 2;
+    // four stages (two tiles of copies in flight) while four CTAs still fit an SM (about 56 KB
+    // each), else three (one tile in flight)
+    td.nstages = smem_for(4) <= 56 * 1024 ? 4 : 3;
     td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
