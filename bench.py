@@ -303,6 +303,11 @@ def main():
 
     # per-kernel split of device time (dominant kernel -> roofline)
     kinds = [p.describe()["kernel"] for _, p, _, _ in items]
+    # a staged tile plan with ragged tiles launches the ragged-tile kernel after the staged kernel
+    launches_per_step = 0
+    for _, p, _, _ in items:
+        t = p.describe().get("tile") or {}
+        launches_per_step += 1 + int(bool(t.get("async")) and t.get("ragged_tiles", 0) > 0)
     per_kind = {}
     for s in range(args.steps):
         for k, (c, plan, A, B) in enumerate(items):
@@ -345,7 +350,7 @@ def main():
                            "l2": "inputs larger than L2 (|A| ~ 200 MiB per case); no flush needed",
                            "parallelism": f"replicas x{world} (independent seeded sweeps, no collective)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "gpu_launches": len(items) * args.steps}
+                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)
     for _, p, _, _ in items:
         p.close()

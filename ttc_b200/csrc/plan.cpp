@@ -883,7 +883,8 @@ std::string plan_describe_json(const ttcb_plan* p) {
     o << ",\"tile\":{\"P\":" << t->P << ",\"LA\":" << t->LA << ",\"LB\":" << t->LB << ",\"ntiles\":" << t->ntiles
       << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
-      << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages << ",\"ext\":[";
+      << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
+      << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
   } else if (p->kernel == TTCB_KERNEL_TILE && p->shape_only) {
