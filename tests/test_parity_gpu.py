@@ -213,3 +213,44 @@ def test_torch_permute_agrees_on_large_sweep_shapes():
         assert torch.equal(B, want), (perm, size, p.describe())
         del A, B, At, want
         torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dtype,beta", [("s", 0.0), ("d", -0.5), ("zc", 0.0)])
+def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta):
+    """Prime extents leave ragged last blocks: the staged kernel moves the complete tiles while the
+    ragged-tile kernel, forked onto a side stream and joined back, moves the rest. The result must
+    equal the oracle when called on the default stream, on a side torch stream, and when the call
+    is captured into a CUDA graph and replayed (the fork and join are captured with it)."""
+    torch = _torch()
+    from ttc_b200 import Plan
+    perm, size = [2, 0, 1], [67, 131, 251]
+    ta, tb = split(dtype)
+    tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
+    A, B = make_inputs(size, perm, dtype, 31)
+    want = oracle.transpose(A, B.copy(), perm, size, 1.5, beta, dtype=dtype)
+    plan = Plan(perm, size, dtype, beta != 0)
+    t = plan.describe()["tile"]
+    assert t["async"] == 1 and t["ragged_tiles"] > 0, t
+    dA = torch.from_numpy(A).cuda()
+    for mode in ("default", "stream", "graph"):
+        dB = torch.from_numpy(B.copy()).cuda()
+        if mode == "default":
+            plan(dA, dB, 1.5, beta)
+        elif mode == "stream":
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                plan(dA, dB, 1.5, beta, s)
+            torch.cuda.current_stream().wait_stream(s)
+        else:
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    plan(dA, dB, 1.5, beta, s)
+            dB.copy_(torch.from_numpy(B))
+            g.replay()
+        torch.cuda.synchronize()
+        assert_bitexact(dB.cpu().numpy(), want, f"{mode} {dtype} beta={beta} tile={t}")
+    plan.close()

@@ -128,6 +128,19 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (td->nrag0 + td->nrag1 > 0) {
         s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_ragged, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
         if (s != TTCB_OK) return s;
+        cudaStream_t side = nullptr;
+        cudaEvent_t fork = nullptr, join = nullptr;
+        if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess)
+          return cuda_fail(e, "cudaStreamCreateWithFlags");
+        p->side_stream = side;
+        if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess)
+          return cuda_fail(e, "cudaEventCreateWithFlags");
+        p->ev_fork = fork;
+        if ((e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming)) != cudaSuccess)
+          return cuda_fail(e, "cudaEventCreateWithFlags");
+        p->ev_join = join;
+        p->fork_mutex = new (std::nothrow) std::mutex();
+        if (!p->fork_mutex) return fail(TTCB_ERR_ALLOC, "host allocation of the plan's mutex failed");
       }
     }
   }
@@ -176,8 +189,7 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
   }
   s = plan_finish_device(p);
   if (s != TTCB_OK) {
-    if (p->dev_desc) cudaFree(p->dev_desc);
-    delete p;
+    ttcb_plan_destroy(p);  // frees whatever the device set-up created
     return s;
   }
   *plan = p;
@@ -187,6 +199,10 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
 void ttcb_plan_destroy(ttcb_plan* plan) {
   if (!plan) return;
   if (plan->dev_desc) cudaFree(plan->dev_desc);
+  if (plan->side_stream) cudaStreamDestroy(static_cast<cudaStream_t>(plan->side_stream));
+  if (plan->ev_fork) cudaEventDestroy(static_cast<cudaEvent_t>(plan->ev_fork));
+  if (plan->ev_join) cudaEventDestroy(static_cast<cudaEvent_t>(plan->ev_join));
+  delete static_cast<std::mutex*>(plan->fork_mutex);
   delete plan;
 }
 
@@ -228,19 +244,32 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
   ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel, va, vb, variant_of(p));
   if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
   if (needs_large_smem(smem)) allow_large_smem(k.func);
-  e = k.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), blocks);
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  if (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG) {
-    // the staged kernel moves complete tiles only; the ragged ones follow on the same stream
-    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
-    if (td->nrag0 + td->nrag1 > 0) {
-      ttcb::KernelRef kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
-      if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
-      if (needs_large_smem(p->smem_ragged)) allow_large_smem(kr.func);
-      e = kr.fn(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream), p->blocks_ragged);
-      if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
-    }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+  const bool ragged = (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG) &&
+                      td->nrag0 + td->nrag1 > 0;
+  if (!ragged) {
+    e = k.fn(p, A, B, alpha, beta, st, blocks);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return TTCB_OK;
   }
+  // The staged kernel moves complete tiles only; the ragged-tile kernel moves the rest, on a side
+  // stream forked from the caller's stream before the staged kernel and joined back after both, so
+  // it runs beside the staged kernel (they write disjoint parts of B) instead of after it.
+  ttcb::KernelRef kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
+  if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
+  if (needs_large_smem(p->smem_ragged)) allow_large_smem(kr.func);
+  cudaStream_t side = static_cast<cudaStream_t>(p->side_stream);
+  cudaEvent_t fork = static_cast<cudaEvent_t>(p->ev_fork), join = static_cast<cudaEvent_t>(p->ev_join);
+  std::lock_guard<std::mutex> lk(*static_cast<std::mutex*>(p->fork_mutex));
+  if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+  e = k.fn(p, A, B, alpha, beta, st, blocks);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  e = kr.fn(p, A, B, alpha, beta, side, p->blocks_ragged);
+  if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
+  if ((e = cudaEventRecord(join, side)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  if ((e = cudaStreamWaitEvent(st, join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
   return TTCB_OK;
 }
 

@@ -46,7 +46,13 @@ struct ttcb_plan {
   int blocks_fast = 0;    // CTAs for the fast tile kernel
   int smem_async = 0;     // staged tile kernel (stages + tables)
   int blocks_async = 0;   // CTAs for the staged tile kernel
-  int blocks_ragged = 0;  // CTAs for the ragged-tile kernel that follows the staged kernel
+  int blocks_ragged = 0;  // CTAs for the ragged-tile kernel that runs beside the staged kernel
+  // the ragged-tile kernel runs on a side stream forked from (and joined back into) the caller's
+  // stream; the mutex keeps one call's record/wait sequence whole when calls come from several threads
+  void* side_stream = nullptr;  // cudaStream_t
+  void* ev_fork = nullptr;      // cudaEvent_t
+  void* ev_join = nullptr;      // cudaEvent_t
+  void* fork_mutex = nullptr;   // std::mutex
   int smem_ragged = 0;    // its dynamic shared memory (two tile buffers + tables)
   int device = 0;
 
