@@ -432,6 +432,13 @@ __global__ void __launch_bounds__(kThreads, 3) tile_fast_kernel(const TileDesc* 
 // beta != 0 the B tile is staged the same way, in B order.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may start
+// while the kernel before it in the stream drains. It lets its own successor start early as soon as
+// every CTA has begun (launch_dependents), and it touches no tensor data before everything the
+// previous kernel wrote is visible (wait). Both are no-ops in a launch without the attribute.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_previous() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 template <int BYTES> __device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
   if constexpr (BYTES == 16)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
@@ -512,6 +519,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
   __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both
   const int tid = threadIdx.x;
+  pdl_allow_next();
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
     reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(desc)[i];
   __syncthreads();
@@ -662,6 +670,8 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   if (tid == 0)
     for (int j = 0; j < D + 2; ++j) decode_into(blockIdx.x + j * G, info[j]);
   __syncthreads();
+  // everything above reads the plan's descriptor only; A and B are touched from here on
+  pdl_wait_previous();
   for (int j = 0; j < D; ++j) {
     issue(info[j], j);
     cp_async_commit();

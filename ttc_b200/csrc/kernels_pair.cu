@@ -61,9 +61,21 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
-  tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG><<<blocks, kThreads, p->smem_async, stream>>>(
-      reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A), static_cast<TB*>(B), al, be);
-  return cudaGetLastError();
+  // programmatic stream serialization: the kernel may start while the previous one in the stream
+  // drains; it waits (griddepcontrol.wait) before it touches A or B
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = p->smem_async;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG>,
+                            reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A),
+                            static_cast<TB*>(B), al, be);
 }
 
 template <int VA, int VB, bool REG>
