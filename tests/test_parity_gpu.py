@@ -215,6 +215,30 @@ def test_torch_permute_agrees_on_large_sweep_shapes():
         torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("perm,size", [([1, 0], [46341, 46341]), ([2, 0, 1], [3, 65537, 10923])])
+def test_more_than_2_to_the_31_elements(perm, size):
+    """Maximum sizes: tensors with more than 2^31 elements (8.6 GB each in fp32) need 64-bit tile
+    bases (TTC used int everywhere). alpha = 1, beta = 0 is a pure permutation, compared with
+    torch.permute(...).contiguous() bit for bit on the GPU."""
+    torch = _torch()
+    from ttc_b200 import Plan
+    n = int(np.prod(size))
+    assert n > 2**31
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    A = torch.rand(n, device="cuda", generator=g)
+    B = torch.empty_like(A)
+    p = Plan(perm, size, "s", False)
+    p(A, B, 1.0, 0.0)
+    nd = len(size)
+    want = A.view(*reversed(size)).permute(*[nd - 1 - perm[j] for j in reversed(range(nd))]).contiguous().view(-1)
+    torch.cuda.synchronize()
+    assert torch.equal(B, want), (perm, size, p.describe())
+    p.close()
+    del A, B, want
+    torch.cuda.empty_cache()
+
+
 @pytest.mark.parametrize("dtype,beta", [("s", 0.0), ("d", -0.5), ("zc", 0.0)])
 def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta):
     """Prime extents leave ragged last blocks: the staged kernel moves the complete tiles while the
