@@ -32,6 +32,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from ttc_b200.replicas import job_throughput, max_over_ranks, rank_seed  # noqa: E402
+
 METRIC = "transpose GB/s (% of HBM peak); learned-vs-searched plan GB/s and tuning time"
 WORKLOAD = ("sweep64: 64 seeded rank-2..6 transpositions, |A|~200 MiB each, fp32/fp64, random "
             "non-identity perms, one extent in [7,31]; even cases alpha=1 beta=0, odd alpha=1.5 beta=-0.5")
@@ -246,7 +248,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    cases = wl.sweep_cases(args.seed + 1000 * rank)[: args.cases]
+    cases = wl.sweep_cases(rank_seed(args.seed, rank))[: args.cases]
     tmap = {"s": torch.float32, "d": torch.float64}
 
     # resident inputs, seeded on the device
@@ -299,13 +301,9 @@ def main():
     for s in range(args.steps):
         step(evs[s])
     torch.cuda.synchronize()
-    elapsed_ms = t0.elapsed_time(t1)
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(t0.elapsed_time(t1), dev)
     ms_per_step = elapsed_ms / args.steps
-    value = bytes_per_step * world / (ms_per_step / 1e3) / 1e9
+    value = job_throughput(bytes_per_step, world, ms_per_step)
 
     # per-kernel split of device time (dominant kernel -> roofline)
     kinds = [p.describe()["kernel"] for _, p, _, _ in items]
@@ -422,12 +420,7 @@ def run_e2e(args, items, stream, dev, world):
         one()
     t1.record(stream)
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1) / args.e2e_steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(t0.elapsed_time(t1) / args.e2e_steps, dev)
     nbytes = sum(p.bytes for _, p, _, _ in sub)
     return {"value": round(nbytes * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "cases": len(sub), "ms_per_step": round(ms, 3),
@@ -536,7 +529,7 @@ def run_batched(args, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    cases = wl.batched_cases(seed=7 + 1000 * rank, count=args.batch_count)
+    cases = wl.batched_cases(seed=rank_seed(7, rank), count=args.batch_count)
     t_tune = time.perf_counter()
     plans, As, Bs, Cs = [], [], [], []
     gen = torch.Generator(device=dev)
@@ -566,12 +559,7 @@ def run_batched(args, rank, world, local):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1) / steps, dev)
 
     def per_call():
         for p, a, cbuf in zip(plans, As, Cs):
