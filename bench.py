@@ -613,7 +613,7 @@ def run_batched(args, rank, world, local):
                 "dtype": "f32", "data": "synthetic (seeded uniform[-1,1])",
                 "config": {"workload": BATCH_WORKLOAD, "problems": len(cases), "bytes_per_step_per_gpu": total,
                            "schedules": ("measured search per problem over tile shape x raster order "
-                                         "(table-driven kernel, 6 candidates, 2 reps)"
+                                         "(staged kernel, 6 candidates, 2 reps)"
                                          if args.batch_tuning == "search" else "planner default"),
                            "tuning_seconds": round(t_tune, 1), "plan_kinds": kinds,
                            "l2": f"{total / 1e9:.2f} GB per step, larger than L2"},

@@ -21,32 +21,68 @@ struct BatchProblem {
 // Batch status codes written by the device (0 = ok).
 enum { kBatchBadItem = 1 };
 
-// One access-width variant of the table-driven tile body as a call of its own: the batch kernel
-// holds four of them and a row path, and separate register allocations keep them from spilling.
-template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM>
-__device__ __noinline__ void batch_tile_body(const TileDesc& d, const TileTables& tt, uint32_t t,
-                                             const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta,
-                                             TA* tile) {
-  tile_body<TA, TB, VA, VB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
+// Complete tiles of a batched tile problem go through a two-buffer asynchronous-copy pipeline: the
+// A tile is copied into shared memory in A order (element p at p + (p / sigmaA) * padA, the plan's
+// staged layout) while the previous tile is written out in B order through the gather table. Each
+// access-width variant is a call of its own, so their register allocations stay separate.
+template <typename TA, int VA>
+__device__ __noinline__ void batch_stage_issue(const TileDesc& d, const int64_t* segA, const TA* __restrict__ At,
+                                               uint32_t stage) {
+  const int P = d.P, LA = d.LA, padA = d.padA;
+  for (int i = threadIdx.x; i < P / VA; i += kThreads) {
+    const int p = i * VA;
+    const int s = (int)fdiv((uint32_t)p, d.divLA);
+    const int sp = (int)fdiv((uint32_t)p, d.divSigmaA);
+    cp_async<VA * sizeof(TA)>(stage + (uint32_t)((p + sp * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+  }
 }
 
-// One tile of a tile problem whose descriptor header (d) and tables (tt) are in shared memory.
+template <typename TA, typename TB, int VB, bool BETA, bool STREAM>
+__device__ __noinline__ void batch_stage_store(const TileDesc& d, const int64_t* segB, const uint16_t* gtab,
+                                               TB* __restrict__ Bt, TA alpha, TB beta, const TA* st) {
+  const int P = d.P, LB = d.LB;
+  constexpr int U = 2;  // B vectors per thread in flight
+  for (int i0 = threadIdx.x; i0 < P / VB; i0 += kThreads * U) {
+    TB* dst[U];
+    Vec<TB, VB> bv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * kThreads;
+      dst[u] = nullptr;
+      if (i < P / VB) {
+        const int q = i * VB;
+        const int s = (int)fdiv((uint32_t)q, d.divLB);
+        dst[u] = Bt + (segB[s] + (q - s * LB));
+        if (BETA) bv[u] = ld_stream<TB, VB>(dst[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!dst[u]) continue;
+      const int q = (i0 + u * kThreads) * VB;
+      uint16_t pos[VB];
+      ld_u16s<TA, VB>(gtab + q, pos);
+      Vec<TB, VB> out;
+#pragma unroll
+      for (int j = 0; j < VB; ++j) {
+        const TA tj = scale_a(alpha, st[pos[j]]);
+        if (BETA)
+          out.v[j] = combine<TA, TB>(tj, bv[u].v[j], beta);
+        else
+          out.v[j] = finish<TA, TB>(tj);
+      }
+      st_vec<TB, VB>(dst[u], out, STREAM);
+    }
+  }
+}
+
+// A ragged tile (last block of a blocked dimension), element-wise, as a call of its own.
 template <typename TA, typename TB, bool BETA, bool STREAM>
-__device__ __forceinline__ void batch_tile(const BatchProblem& bp, const TileDesc& d, const TileTables& tt, uint32_t t,
-                                           TA alpha, TB beta, TA* tile) {
-  const TA* A = static_cast<const TA*>(bp.A);
-  TB* B = static_cast<TB*>(bp.B);
-  constexpr int MA = 16 / sizeof(TA);
-  constexpr int MB = 16 / sizeof(TB);
-  // the widest access each side allows (16 bytes) or scalar; narrower plans run scalar here
-  if (bp.va == MA && bp.vb == MB)
-    batch_tile_body<TA, TB, MA, MB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-  else if (bp.va == MA)
-    batch_tile_body<TA, TB, MA, 1, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-  else if (bp.vb == MB)
-    batch_tile_body<TA, TB, 1, MB, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
-  else
-    batch_tile_body<TA, TB, 1, 1, BETA, STREAM>(d, tt, t, A, B, alpha, beta, tile);
+__device__ __noinline__ void batch_ragged(const TileDesc& d, TileTables tt, int lim0, int lim1,
+                                          const TA* __restrict__ At, TB* __restrict__ Bt, TA alpha, TB beta,
+                                          TA* tile) {
+  const int lim[2] = {lim0, lim1};
+  tile_ragged<TA, TB, BETA, STREAM>(d, tt, lim, At, Bt, alpha, beta, tile);
 }
 
 template <typename TA, typename TB, bool BETA, bool STREAM>
@@ -68,21 +104,50 @@ __device__ __forceinline__ void batch_row(const BatchProblem& bp, uint32_t item,
 
 // counter[0]: next work item (zeroed before every launch); status[0]: first error code.
 // A CTA claims `chunk` consecutive items per atomic and walks them in order; the problem index
-// advances along the prefix array. A tile problem's descriptor header and run tables are copied
-// into shared memory (after the `slots_bytes` tile buffer) when the CTA moves to it.
+// advances along the prefix array. When it moves to a tile problem it copies that problem's
+// descriptor header and run and gather tables into shared memory (after two stage buffers of
+// `slots_bytes` each) and pipelines the problem's consecutive complete tiles.
 template <typename TA, typename TB, bool BETA, bool STREAM>
 __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* __restrict__ probs,
                                                          const int64_t* __restrict__ prefix, int count,
                                                          unsigned long long total, unsigned long long* counter,
                                                          int* status, TA alpha, TB beta, int slots_bytes, int chunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TA* tile = reinterpret_cast<TA*>(smem_raw);
   __shared__ TileDesc d;
   __shared__ unsigned long long s_item;
   __shared__ int s_prob;
-  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + slots_bytes);
+  constexpr int MA = 16 / sizeof(TA);
+  constexpr int MB = 16 / sizeof(TB);
+  const uint32_t stage0 = smem_u32(smem_raw);
+  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + 2 * slots_bytes);
+  int64_t* segB = segA;
+  uint16_t* gtab = nullptr;
   int cur = -1;  // problem whose header and tables are in shared memory
-  TileTables tt{nullptr, nullptr, nullptr};
+  const BatchProblem* bp = nullptr;
+  // the complete tile whose copies are in flight: its B base and its buffer
+  bool have = false;
+  int64_t pend_bB = 0;
+  int pend_buf = 0;
+
+  auto store_pending = [&](bool newer_in_flight) {
+    if (newer_in_flight)
+      cp_async_wait<1>();
+    else
+      cp_async_wait<0>();
+    __syncthreads();
+    TB* Bt = static_cast<TB*>(bp->B) + pend_bB;
+    const TA* st = reinterpret_cast<const TA*>(smem_raw + pend_buf * slots_bytes);
+    if (bp->vb == MB)
+      batch_stage_store<TA, TB, MB, BETA, STREAM>(d, segB, gtab, Bt, alpha, beta, st);
+    else
+      batch_stage_store<TA, TB, 1, BETA, STREAM>(d, segB, gtab, Bt, alpha, beta, st);
+    __syncthreads();
+  };
+  auto flush = [&]() {
+    if (have) store_pending(false);
+    have = false;
+  };
+
   for (;;) {
     if (threadIdx.x == 0) {
       const unsigned long long it = atomicAdd(counter, (unsigned long long)chunk);
@@ -115,31 +180,52 @@ __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* 
         if (threadIdx.x == 0) atomicCAS(status, 0, (int)kBatchBadItem);
         continue;
       }
-      const BatchProblem& bp = probs[pr];
-      if (bp.kind == TTCB_KERNEL_TILE) {
-        if (pr != cur) {
-          // the previous tile ended with a barrier, so the old header and tables are free
-          const TileDesc* gd = reinterpret_cast<const TileDesc*>(bp.desc);
-          for (int i = threadIdx.x; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
-            reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(gd)[i];
-          __syncthreads();
-          int64_t* sB = segA + d.nsegA;
-          uint16_t* pt = reinterpret_cast<uint16_t*>(sB + d.nsegB);
-          const int64_t* gA = reinterpret_cast<const int64_t*>(bp.desc + d.off_segA);
-          const int64_t* gB = reinterpret_cast<const int64_t*>(bp.desc + d.off_segB);
-          const uint32_t* gP = reinterpret_cast<const uint32_t*>(bp.desc + d.off_perm);
-          for (int i = threadIdx.x; i < d.nsegA; i += kThreads) segA[i] = gA[i];
-          for (int i = threadIdx.x; i < d.nsegB; i += kThreads) sB[i] = gB[i];
-          for (int i = threadIdx.x; i < (d.P + 1) / 2; i += kThreads) reinterpret_cast<uint32_t*>(pt)[i] = gP[i];
-          __syncthreads();
-          tt = TileTables{segA, sB, pt};
-          cur = pr;
-        }
-        batch_tile<TA, TB, BETA, STREAM>(bp, d, tt, local, alpha, beta, tile);
+      if (probs[pr].kind != TTCB_KERNEL_TILE) {
+        flush();
+        batch_row<TA, TB, BETA, STREAM>(probs[pr], local, alpha, beta);
+        continue;
+      }
+      if (pr != cur) {
+        flush();  // the pending tile belongs to the previous problem and its tables
+        bp = &probs[pr];
+        const TileDesc* gd = reinterpret_cast<const TileDesc*>(bp->desc);
+        for (int i = threadIdx.x; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
+          reinterpret_cast<uint32_t*>(&d)[i] = reinterpret_cast<const uint32_t*>(gd)[i];
+        __syncthreads();
+        segB = segA + d.nsegA;
+        gtab = reinterpret_cast<uint16_t*>(segB + d.nsegB);
+        const int64_t* gA = reinterpret_cast<const int64_t*>(bp->desc + d.off_segA);
+        const int64_t* gB = reinterpret_cast<const int64_t*>(bp->desc + d.off_segB);
+        const uint32_t* gG = reinterpret_cast<const uint32_t*>(bp->desc + d.off_gtab);
+        for (int i = threadIdx.x; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+        for (int i = threadIdx.x; i < d.nsegB; i += kThreads) segB[i] = gB[i];
+        for (int i = threadIdx.x; i < (d.P + 1) / 2; i += kThreads) reinterpret_cast<uint32_t*>(gtab)[i] = gG[i];
+        __syncthreads();
+        cur = pr;
+      }
+      int64_t bA, bB;
+      int lim[2];
+      const bool full = decode_tile(d, local, bA, bB, lim);
+      const TA* A = static_cast<const TA*>(bp->A);
+      if (full) {
+        const int b = have ? (pend_buf ^ 1) : 0;
+        if (bp->va == MA)
+          batch_stage_issue<TA, MA>(d, segA, A + bA, stage0 + b * slots_bytes);
+        else
+          batch_stage_issue<TA, 1>(d, segA, A + bA, stage0 + b * slots_bytes);
+        cp_async_commit();
+        if (have) store_pending(true);
+        have = true;
+        pend_bB = bB;
+        pend_buf = b;
       } else {
-        batch_row<TA, TB, BETA, STREAM>(bp, local, alpha, beta);
+        flush();
+        const TileTables tt{segA, segB, reinterpret_cast<const uint16_t*>(bp->desc + d.off_perm)};
+        batch_ragged<TA, TB, BETA, STREAM>(d, tt, lim[0], lim[1], A + bA, static_cast<TB*>(bp->B) + bB, alpha, beta,
+                                           reinterpret_cast<TA*>(smem_raw));
       }
     }
+    flush();
   }
 }
 

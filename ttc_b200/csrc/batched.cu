@@ -47,8 +47,8 @@ struct ttcb_batch {
   int64_t bytes = 0;
   unsigned long long total = 0;
   int blocks = 0;
-  int smem = 0;         // tile buffer + the largest problem's tables
-  int slots_bytes = 0;  // tile buffer (the tables follow it)
+  int smem = 0;         // two stage buffers + the largest problem's tables
+  int slots_bytes = 0;  // one stage buffer (the largest staged tile)
   int chunk = 1;        // items claimed per atomic
   void* d_probs = nullptr;
   int64_t* d_prefix = nullptr;
@@ -160,7 +160,9 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
       } else {
         const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
         items = td->ntiles;
-        max_slots_bytes = std::max<int>(max_slots_bytes, (int)ttcb::tile_slots_bytes(td->phys_size, EA));
+        // one stage buffer: the staged layout (or, for a ragged tile, the slots), 16-byte aligned
+        max_slots_bytes = std::max<int>(
+            max_slots_bytes, (int)ttcb::al16((size_t)std::max(td->stage_elems, td->phys_size) * EA));
         max_table_bytes = std::max<int>(max_table_bytes, 8 * (td->nsegA + td->nsegB) + 4 * ((td->P + 1) / 2));
       }
       b->bytes += ttcb_plan_bytes(p);
@@ -169,7 +171,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
   }
   b->total = (unsigned long long)prefix[count];
   b->slots_bytes = (int)((max_slots_bytes + 15) & ~15);
-  b->smem = b->slots_bytes + max_table_bytes;
+  b->smem = 2 * b->slots_bytes + max_table_bytes;  // two stage buffers, then the tables
 
   // device copies
   if ((e = cudaMalloc(&b->d_desc, hdesc.size())) != cudaSuccess ||
