@@ -209,8 +209,10 @@ def batch_space(dtype: str) -> dict:
     """The knobs that matter inside the batched kernel: tile shape and raster order (it runs every
     complete tile through the staged asynchronous-copy layout on its own persistent grid, so the
     CTA count of a plain launch does not apply; candidates are timed with the staged kernel)."""
-    s = knob_space(dtype)
-    return {"tile_elems": s["tile_elems"], "run_bytes": s["run_bytes"], "tile_variant": [3],
+    base = 16384 // ELEM_BYTES[split_dtype(dtype)[0]]
+    # tiles of at most half the default size: the batch's shared memory (and so its CTAs per SM) is
+    # sized for its largest tile
+    return {"tile_elems": [base // 4, base // 2], "run_bytes": [0, 256, 1024], "tile_variant": [3],
             "loop_order": [0, 1], "blocks": [0]}
 
 

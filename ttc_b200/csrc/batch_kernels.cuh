@@ -18,6 +18,14 @@ struct BatchProblem {
   int32_t pad_;
 };
 
+// Stage buffers of the batched kernel's tile pipeline (tiles in flight ahead of the one written out:
+// kBatchStages - 1).
+#ifndef TTCB_BATCH_STAGES
+#define TTCB_BATCH_STAGES 2
+#endif
+constexpr int kBatchStages = TTCB_BATCH_STAGES;
+static_assert(kBatchStages == 2 || kBatchStages == 3, "the pending-tile queue holds at most two tiles");
+
 // Batch status codes written by the device (0 = ok).
 enum { kBatchBadItem = 1 };
 
@@ -105,8 +113,8 @@ __device__ __forceinline__ void batch_row(const BatchProblem& bp, uint32_t item,
 // counter[0]: next work item (zeroed before every launch); status[0]: first error code.
 // A CTA claims `chunk` consecutive items per atomic and walks them in order; the problem index
 // advances along the prefix array. When it moves to a tile problem it copies that problem's
-// descriptor header and run and gather tables into shared memory (after two stage buffers of
-// `slots_bytes` each) and pipelines the problem's consecutive complete tiles.
+// descriptor header and run and gather tables into shared memory (after kBatchStages stage buffers
+// of `slots_bytes` each) and pipelines the problem's consecutive complete tiles.
 template <typename TA, typename TB, bool BETA, bool STREAM>
 __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* __restrict__ probs,
                                                          const int64_t* __restrict__ prefix, int count,
@@ -119,33 +127,40 @@ __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* 
   constexpr int MA = 16 / sizeof(TA);
   constexpr int MB = 16 / sizeof(TB);
   const uint32_t stage0 = smem_u32(smem_raw);
-  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + 2 * slots_bytes);
+  int64_t* segA = reinterpret_cast<int64_t*>(smem_raw + kBatchStages * slots_bytes);
   int64_t* segB = segA;
   uint16_t* gtab = nullptr;
   int cur = -1;  // problem whose header and tables are in shared memory
   const BatchProblem* bp = nullptr;
-  // the complete tile whose copies are in flight: its B base and its buffer
-  bool have = false;
-  int64_t pend_bB = 0;
-  int pend_buf = 0;
+  // complete tiles whose copies are in flight, oldest first (at most kBatchStages - 1): B base and
+  // stage buffer of each
+  int npend = 0, next_buf = 0;
+  int64_t pend_bB[2] = {0, 0};
+  int pend_buf[2] = {0, 0};
 
-  auto store_pending = [&](bool newer_in_flight) {
-    if (newer_in_flight)
+  // writes out the oldest pending tile once its copies (and no newer ones: `newer` stay in flight)
+  // have landed
+  auto store_oldest = [&](int newer) {
+    if (newer >= 2)
+      cp_async_wait<2>();
+    else if (newer == 1)
       cp_async_wait<1>();
     else
       cp_async_wait<0>();
     __syncthreads();
-    TB* Bt = static_cast<TB*>(bp->B) + pend_bB;
-    const TA* st = reinterpret_cast<const TA*>(smem_raw + pend_buf * slots_bytes);
+    TB* Bt = static_cast<TB*>(bp->B) + pend_bB[0];
+    const TA* st = reinterpret_cast<const TA*>(smem_raw + pend_buf[0] * slots_bytes);
     if (bp->vb == MB)
       batch_stage_store<TA, TB, MB, BETA, STREAM>(d, segB, gtab, Bt, alpha, beta, st);
     else
       batch_stage_store<TA, TB, 1, BETA, STREAM>(d, segB, gtab, Bt, alpha, beta, st);
     __syncthreads();
+    pend_bB[0] = pend_bB[1];
+    pend_buf[0] = pend_buf[1];
+    --npend;
   };
   auto flush = [&]() {
-    if (have) store_pending(false);
-    have = false;
+    while (npend > 0) store_oldest(npend - 1);
   };
 
   for (;;) {
@@ -208,16 +223,24 @@ __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* 
       const bool full = decode_tile(d, local, bA, bB, lim);
       const TA* A = static_cast<const TA*>(bp->A);
       if (full) {
-        const int b = have ? (pend_buf ^ 1) : 0;
+        // the buffer after the newest pending one is free: its previous tile was written out
+        // (followed by a barrier) before the pipeline last held kBatchStages - 1 tiles
+        const int b = next_buf;
+        next_buf = next_buf + 1 == kBatchStages ? 0 : next_buf + 1;
         if (bp->va == MA)
           batch_stage_issue<TA, MA>(d, segA, A + bA, stage0 + b * slots_bytes);
         else
           batch_stage_issue<TA, 1>(d, segA, A + bA, stage0 + b * slots_bytes);
         cp_async_commit();
-        if (have) store_pending(true);
-        have = true;
-        pend_bB = bB;
-        pend_buf = b;
+        if (npend == kBatchStages - 1) store_oldest(kBatchStages - 1);
+        if (npend == 0) {  // constant indices keep the queue in registers
+          pend_bB[0] = bB;
+          pend_buf[0] = b;
+        } else {
+          pend_bB[1] = bB;
+          pend_buf[1] = b;
+        }
+        ++npend;
       } else {
         flush();
         const TileTables tt{segA, segB, reinterpret_cast<const uint16_t*>(bp->desc + d.off_perm)};

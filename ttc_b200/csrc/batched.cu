@@ -47,7 +47,7 @@ struct ttcb_batch {
   int64_t bytes = 0;
   unsigned long long total = 0;
   int blocks = 0;
-  int smem = 0;         // two stage buffers + the largest problem's tables
+  int smem = 0;         // the stage buffers + the largest problem's tables
   int slots_bytes = 0;  // one stage buffer (the largest staged tile)
   int chunk = 1;        // items claimed per atomic
   void* d_probs = nullptr;
@@ -171,7 +171,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
   }
   b->total = (unsigned long long)prefix[count];
   b->slots_bytes = (int)((max_slots_bytes + 15) & ~15);
-  b->smem = 2 * b->slots_bytes + max_table_bytes;  // two stage buffers, then the tables
+  b->smem = ttcb::kBatchStages * b->slots_bytes + max_table_bytes;  // stage buffers, then the tables
 
   // device copies
   if ((e = cudaMalloc(&b->d_desc, hdesc.size())) != cudaSuccess ||
