@@ -317,11 +317,8 @@ def main():
 
     # per-kernel split of device time (dominant kernel -> roofline)
     kinds = [p.describe()["kernel"] for _, p, _, _ in items]
-    # a staged tile plan with ragged tiles launches the ragged-tile kernel after the staged kernel
-    launches_per_step = 0
-    for _, p, _, _ in items:
-        t = p.describe().get("tile") or {}
-        launches_per_step += 1 + int(bool(t.get("async")) and t.get("ragged_tiles", 0) > 0)
+    # a staged tile plan with ragged tiles also launches its edge plans (or the ragged-tile kernel)
+    launches_per_step = sum(p.launches() for _, p, _, _ in items)
     per_kind = {}
     for s in range(args.steps):
         for k, (c, plan, A, B) in enumerate(items):

@@ -68,7 +68,10 @@ typedef struct {
   int32_t streaming;     /* 0 = default (streaming stores when beta == 0), 1 = on, -1 = off     */
   int32_t tile_variant;  /* tile kernel: 0 auto, 1 table-driven, 2 register-resident prefetch,
                             3 staged asynchronous copies                                        */
-  int32_t reserved[8];
+  int32_t ragged;        /* staged tile kernel's ragged tiles (last blocks of dimensions that
+                            the tile does not divide): 0 = planned as transpositions of their
+                            own and moved by the staged kernel, 1 = element-wise kernel         */
+  int32_t reserved[7];
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

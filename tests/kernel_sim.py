@@ -45,6 +45,22 @@ def host_desc(perm, size, dtype="s", beta=False, lda=None, ldb=None, tuning=None
     return kind.value, buf.raw
 
 
+def edge_boxes(perm, size, dtype="s", beta=False, lda=None, ldb=None, tuning=None):
+    """The boxes a plan's ragged tiles are moved as (edge plans), from the host-only planner."""
+    import json
+    ta, tb = (dtype[0], dtype[1]) if len(dtype) == 2 else (dtype, dtype)
+    if isinstance(tuning, dict):
+        tuning = Tuning.make(**tuning)
+    args = (len(size), i32(perm), i64(size), i64(lda) if lda else None, i64(ldb) if ldb else None,
+            _native.DTYPES[ta], _native.DTYPES[tb], int(beta), ctypes.byref(tuning) if tuning else None)
+    n = _native.lib().ttcb_test_plan_edges(*args, None, 0)
+    if n == 0:
+        raise _native.TTCError(1, _native.last_error())
+    buf = ctypes.create_string_buffer(n)
+    _native.lib().ttcb_test_plan_edges(*args, buf, n)
+    return json.loads(buf.value.decode())
+
+
 def _i32(b, off):
     return int(np.frombuffer(b, dtype=np.int32, count=1, offset=off)[0])
 
@@ -123,8 +139,9 @@ def parse_row(b):
     return r
 
 
-def simulate_tile(t):
-    """Returns arrays (a_off, b_off): for every element written, the A element read."""
+def simulate_tile(t, split=False):
+    """Returns arrays (a_off, b_off): for every element written, the A element read. With split,
+    returns them for the complete tiles and for the ragged tiles separately."""
     P = t["P"]
     p = np.arange(P, dtype=np.int64)
     q = np.arange(P, dtype=np.int64)
@@ -139,6 +156,7 @@ def simulate_tile(t):
     assert set(t["ptab"].tolist()) == set(slot_q.tolist()), "load and store slots differ"
     a_out, b_out = [], []
     ragged = []
+    is_rag = []
     for tile in range(t["ntiles"]):
         rem = tile
         bA = bB = 0
@@ -169,6 +187,7 @@ def simulate_tile(t):
         assert (src >= 0).all(), "store phase reads a slot the load phase did not write"
         a_out.append(src)
         b_out.append(bB + b_rel[okB])
+        is_rag.append(bool(ragged) and ragged[-1] == tile)
     # the staged kernel walks the complete tiles, numbered over the divf counts
     full = []
     for tf in range(t["nfull"]):
@@ -185,6 +204,11 @@ def simulate_tile(t):
     got = [ragged_tile_index(t, r) for r in range(t["nrag0"] + t["nrag1"])]
     assert len(got) == len(set(got)), "a ragged tile is enumerated twice"
     assert sorted(got) == want, "ragged-tile enumeration differs from the ragged tiles"
+    if split:
+        def cat(xs, keep):
+            xs = [x for x, k in zip(xs, is_rag) if k == keep]
+            return np.concatenate(xs) if xs else np.zeros(0, np.int64)
+        return (cat(a_out, False), cat(b_out, False)), (cat(a_out, True), cat(b_out, True))
     return np.concatenate(a_out) if a_out else np.zeros(0, np.int64), \
         np.concatenate(b_out) if b_out else np.zeros(0, np.int64)
 

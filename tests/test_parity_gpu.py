@@ -239,12 +239,15 @@ def test_more_than_2_to_the_31_elements(perm, size):
     torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("ragged", [0, 1])
 @pytest.mark.parametrize("dtype,beta", [("s", 0.0), ("d", -0.5), ("zc", 0.0)])
-def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta):
+def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta, ragged):
     """Prime extents leave ragged last blocks: the staged kernel moves the complete tiles while the
-    ragged-tile kernel, forked onto a side stream and joined back, moves the rest. The result must
-    equal the oracle when called on the default stream, on a side torch stream, and when the call
-    is captured into a CUDA graph and replayed (the fork and join are captured with it)."""
+    side stream, forked from the caller's stream and joined back, moves the rest - as edge plans
+    (the ragged boxes planned as transpositions of their own, offset into A and B) or, with the
+    `ragged` knob at 1, with the element-wise ragged-tile kernel. The result must equal the oracle
+    when called on the default stream, on a side torch stream, and when the call is captured into
+    a CUDA graph and replayed (the fork and join are captured with it)."""
     torch = _torch()
     from ttc_b200 import Plan
     perm, size = [2, 0, 1], [67, 131, 251]
@@ -252,9 +255,11 @@ def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta):
     tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
     A, B = make_inputs(size, perm, dtype, 31)
     want = oracle.transpose(A, B.copy(), perm, size, 1.5, beta, dtype=dtype)
-    plan = Plan(perm, size, dtype, beta != 0)
-    t = plan.describe()["tile"]
+    plan = Plan(perm, size, dtype, beta != 0, tuning={"ragged": ragged})
+    d = plan.describe()
+    t = d["tile"]
     assert t["async"] == 1 and t["ragged_tiles"] > 0, t
+    assert bool(d.get("edges")) == (ragged == 0), d
     dA = torch.from_numpy(A).cuda()
     for mode in ("default", "stream", "graph"):
         dB = torch.from_numpy(B.copy()).cuda()
@@ -278,3 +283,35 @@ def test_ragged_tiles_beside_the_staged_kernel_streams_and_graphs(dtype, beta):
         torch.cuda.synchronize()
         assert_bitexact(dB.cpu().numpy(), want, f"{mode} {dtype} beta={beta} tile={t}")
     plan.close()
+
+
+@pytest.mark.parametrize("offset", [0, 1])
+def test_edge_plans_random_ragged_problems(offset):
+    """Problems whose tiles leave ragged last blocks (prime extents), with padded lda/ldb, a unit
+    first dimension with a padded leading dimension (the edge boxes then start with a unit
+    dimension), mixed and complex types, beta != 0 and misaligned base pointers: the edge plans
+    (offset sub-problems moved by the staged kernel on the side stream) must give the oracle's
+    result bit for bit."""
+    rng = np.random.default_rng(23 + offset)
+    primes = [3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67]
+    with_edges = 0
+    for it in range(48):
+        r = int(rng.integers(2, 6))
+        size = [int(rng.choice(primes)) for _ in range(r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        while perm == sorted(perm):
+            perm = [int(x) for x in rng.permutation(r)]
+        lda = ldb = None
+        if it % 3 == 1:
+            lda = [s + int(rng.integers(0, 3)) for s in size]
+            ldb = [size[perm[j]] + int(rng.integers(0, 3)) for j in range(r)]
+        if it % 4 == 2:
+            size, perm = [1] + size, [0] + [x + 1 for x in perm]
+            lda = [2] + (lda or size[1:])
+            ldb = [1] + (ldb or [size[perm[j]] for j in range(1, r + 1)])
+        dtype = ["s", "d", "zc", "ds", "c"][it % 5]
+        beta = [0.0, -0.5][it % 2]
+        tuning = {"tile_elems": [0, 256, 512][it % 3]} if it % 3 else None
+        desc = check_case(perm, size, dtype, 1.5, beta, lda, ldb, tuning, seed=100 + it, offset=offset)
+        with_edges += bool(desc.get("edges"))
+    assert with_edges >= 12, with_edges

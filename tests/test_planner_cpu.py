@@ -212,3 +212,62 @@ def test_ragged_tile_enumeration_covers_every_ragged_tile_once():
                 seen_one += 1
                 seen_two += t["nrag1"] > 0
     assert seen_one > 100 and seen_two > 5
+
+
+def _pairs(a, b):
+    return np.stack([np.asarray(a, np.int64), np.asarray(b, np.int64)], 1)
+
+
+def test_edge_plans_move_exactly_the_ragged_tiles():
+    """A plan's ragged tiles are moved as one or two boxes planned as transpositions of their own
+    (edge plans, offset into A and B). Replaying each box's own plan must give exactly the element
+    pairs (A read, B written) of the parent's ragged tiles, each once - with padded leading
+    dimensions and a first fused stride other than 1 (a unit leading dimension in the box)."""
+    rng = np.random.default_rng(11)
+    primes = [2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53]
+    checked = two = lead = 0
+    for it in range(400):
+        r = int(rng.integers(2, 6))
+        size = [int(rng.choice(primes)) for _ in range(r)]
+        perm = [int(x) for x in rng.permutation(r)]
+        lda = ldb = None
+        if it % 3 == 1:
+            lda = [s + int(rng.integers(0, 3)) for s in size]
+            ldb = [size[perm[j]] + int(rng.integers(0, 3)) for j in range(r)]
+        if it % 5 == 2:
+            # a unit first dimension with a padded leading dimension: fused stride 1 != 1
+            size, perm = [1] + size, [0] + [x + 1 for x in perm]
+            lda = [3] + (lda or size[1:])
+            ldb = [1] + (ldb or [size[perm[j]] for j in range(1, r + 1)])
+            r += 1
+        dtype = ["s", "d", "zc"][it % 3]
+        for tu in (None, {"tile_elems": 256}):
+            try:
+                kind, b = kernel_sim.host_desc(perm, size, dtype, False, lda, ldb, tu)
+            except TTCError:
+                continue
+            if kind != 1:
+                continue
+            t = kernel_sim.parse_tile(b)
+            if t["nrag0"] == 0 or t["ntiles"] > 3000:
+                continue
+            (af, bf), (ar, br) = kernel_sim.simulate_tile(t, split=True)
+            boxes = kernel_sim.edge_boxes(perm, size, dtype, False, lda, ldb, tu)
+            assert len(boxes) == 1 + (t["nrag1"] > 0), boxes
+            ea, eb = [], []
+            for bx in boxes:
+                assert all(bx["lda"][i] >= bx["size"][i] for i in range(bx["rank"]))
+                assert all(bx["ldb"][j] >= bx["size"][bx["perm"][j]] for j in range(bx["rank"]))
+                k2, (a2, b2) = kernel_sim.simulate(bx["perm"], bx["size"], dtype, False, bx["lda"], bx["ldb"])
+                ea.append(a2 + bx["offA"])
+                eb.append(b2 + bx["offB"])
+                lead += bx["rank"] > len([s for s in size if s > 1]) and bx["size"][0] == 1
+            got = _pairs(np.concatenate(ea), np.concatenate(eb))
+            want = _pairs(ar, br)
+            assert len(np.unique(got[:, 1])) == len(got), "an edge plan writes a B element twice"
+            got = got[np.lexsort(got.T[::-1])]
+            want = want[np.lexsort(want.T[::-1])]
+            assert np.array_equal(got, want), (perm, size, lda, ldb, dtype, tu, boxes)
+            checked += 1
+            two += len(boxes) == 2
+    assert checked > 100 and two > 5 and lead > 0, (checked, two, lead)

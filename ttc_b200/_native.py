@@ -34,7 +34,8 @@ class TTCError(RuntimeError):
 class Tuning(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("tile_elems", ctypes.c_int32), ("run_bytes", ctypes.c_int32),
                 ("vec", ctypes.c_int32), ("blocks", ctypes.c_int32), ("loop_order", ctypes.c_int32),
-                ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
+                ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("ragged", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":
@@ -85,6 +86,8 @@ TEST_SYMBOLS = [
     ("ttcb_test_plan_shapes", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_int, ctypes.c_char_p,
                                                 ctypes.c_size_t]),
+    ("ttcb_test_plan_edges", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_char_p, ctypes.c_size_t]),
 ]
 
 

@@ -117,6 +117,10 @@ class Plan:
         lib().ttcb_plan_describe(self._h, buf, n)
         return json.loads(buf.value.decode())
 
+    def launches(self) -> int:
+        """Kernels one call launches (with 16-byte aligned tensors): see `describe_launches`."""
+        return describe_launches(self.describe())
+
     @property
     def bytes(self) -> int:
         """Algorithmic bytes per call: N*(|TA| + |TB|*(1+[beta!=0]))."""
@@ -155,6 +159,17 @@ def transpose(A, B, perm: Sequence[int], size: Optional[Sequence[int]] = None, a
         plan = Plan(perm, size, dtype, complex(beta) != 0, lda, ldb, tuning)
         _plan_cache[key] = plan
     plan(A, B, alpha, beta, stream)
+
+
+def describe_launches(d: dict) -> int:
+    """Kernels a call of the plan described by `d` launches: its kernel, and for a staged tile plan
+    with ragged tiles either its edge plans' kernels or the element-wise ragged-tile kernel."""
+    t = d.get("tile") or {}
+    n = 1
+    if t.get("async") and t.get("ragged_tiles", 0) > 0 and d.get("tile_variant", 0) in (0, 3):
+        edges = d.get("edges") or []
+        n += sum(describe_launches(e["plan"]) for e in edges) if edges else 1
+    return n
 
 
 def plan_host_json(perm, size, dtype="s", beta_nonzero=False, lda=None, ldb=None, tuning=None) -> dict:

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <sstream>
 #include <vector>
 #include <new>
 #include <string>
@@ -128,6 +129,7 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (td->nrag0 + td->nrag1 > 0) {
         s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_ragged, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
         if (s != TTCB_OK) return s;
+        if (p->depth > 0) return TTCB_OK;  // an edge plan runs on its parent's side stream
         cudaStream_t side = nullptr;
         cudaEvent_t fork = nullptr, join = nullptr;
         if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess)
@@ -145,6 +147,124 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     }
   }
   return TTCB_OK;
+}
+
+// Launches a checked plan on stream st. The staged kernel moves complete tiles only; a plan with
+// ragged tiles forks its side stream from st before the staged kernel and joins it back after, and
+// the side stream moves the ragged tiles beside the staged kernel (they write disjoint parts of B):
+// through the edge plans when there are some, else with the element-wise ragged-tile kernel. An
+// edge plan with ragged tiles of its own runs its ragged-tile kernel after its staged kernel.
+static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
+                               cudaStream_t st) {
+  const int EA = dtype_bytes(p->ta), EB = dtype_bytes(p->tb);
+  cudaError_t e;
+  int va = p->vecA, vb = p->vecB;
+  while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
+  while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
+  if (p->kernel == TTCB_KERNEL_ROW) va = vb = std::min(va, vb);
+  int kernel = p->kernel, blocks = p->blocks, smem = p->smem_bytes;
+  if (kernel == TTCB_KERNEL_TILE) {
+    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    const int want = p->tuning.tile_variant;
+    const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
+    if ((want == 0 || want == 3) && td->async_ok) {
+      kernel = (fast_ok && td->reg_ok) ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
+      blocks = p->blocks_async;
+      smem = p->smem_async;
+    } else if ((want == 0 || want == 2) && fast_ok) {
+      kernel = TTCB_KERNEL_TILE_FAST;
+      blocks = p->blocks_fast;
+      smem = p->smem_fast;
+    }
+  }
+  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel, va, vb, variant_of(p));
+  if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
+  if (needs_large_smem(smem)) allow_large_smem(k.func);
+  const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+  const bool ragged = (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG) &&
+                      td->nrag0 + td->nrag1 > 0;
+  if (!ragged) {
+    e = k.fn(p, A, B, alpha, beta, st, blocks);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return TTCB_OK;
+  }
+  ttcb::KernelRef kr{};
+  if (p->nedge == 0) {
+    kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
+    if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
+    if (needs_large_smem(p->smem_ragged)) allow_large_smem(kr.func);
+  }
+  if (p->depth > 0) {
+    e = k.fn(p, A, B, alpha, beta, st, blocks);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    e = kr.fn(p, A, B, alpha, beta, st, p->blocks_ragged);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
+    return TTCB_OK;
+  }
+  cudaStream_t side = static_cast<cudaStream_t>(p->side_stream);
+  cudaEvent_t fork = static_cast<cudaEvent_t>(p->ev_fork), join = static_cast<cudaEvent_t>(p->ev_join);
+  std::lock_guard<std::mutex> lk(*static_cast<std::mutex*>(p->fork_mutex));
+  if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+  e = k.fn(p, A, B, alpha, beta, st, blocks);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  if (p->nedge > 0) {
+    for (int j = 0; j < p->nedge; ++j) {
+      const ttcb_plan* q = p->edge[j];
+      ttcb_status s = launch_plan(q, static_cast<const char*>(A) + q->base_offA * EA,
+                                  static_cast<char*>(B) + q->base_offB * EB, alpha, beta, side);
+      if (s != TTCB_OK) return s;
+    }
+  } else {
+    e = kr.fn(p, A, B, alpha, beta, side, p->blocks_ragged);
+    if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
+  }
+  if ((e = cudaEventRecord(join, side)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  if ((e = cudaStreamWaitEvent(st, join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+  return TTCB_OK;
+}
+
+// Edge plans: the boxes of a staged-kernel plan's ragged tiles, each planned as a transposition of
+// its own (default schedule, the caller's streaming choice) so that the staged kernel moves them
+// too. A box that cannot be planned leaves all of them to the element-wise ragged-tile kernel.
+static void plan_create_edges(ttcb_plan* p) {
+  if (p->depth > 0 || p->empty || p->kernel != TTCB_KERNEL_TILE || p->tuning.ragged == 1) return;
+  if (p->tuning.tile_variant == 1 || p->tuning.tile_variant == 2) return;  // kernels without ragged split
+  const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+  if (!td->async_ok || td->nrag0 + td->nrag1 == 0) return;
+  EdgeBox box[2];
+  const int n = plan_edge_boxes(p, box);
+  if (n <= 0) return;
+  for (int k = 0; k < n; ++k) {
+    ttcb_plan* q = new (std::nothrow) ttcb_plan();
+    if (!q) break;
+    q->rank = box[k].rank;
+    for (int i = 0; i < q->rank; ++i) {
+      q->perm[i] = box[k].perm[i];
+      q->size[i] = box[k].size[i];
+      q->lda[i] = box[k].lda[i];
+      q->ldb[i] = box[k].ldb[i];
+    }
+    q->ta = p->ta;
+    q->tb = p->tb;
+    q->beta_nonzero = p->beta_nonzero;
+    q->tuning.streaming = p->tuning.streaming;
+    q->depth = 1;
+    q->base_offA = box[k].offA;
+    q->base_offB = box[k].offB;
+    std::string err;
+    if (plan_build_host(q, err) != TTCB_OK || plan_finish_device(q) != TTCB_OK) {
+      ttcb_plan_destroy(q);
+      break;
+    }
+    p->edge[p->nedge++] = q;
+  }
+  if (p->nedge != n) {
+    for (int k = 0; k < p->nedge; ++k) ttcb_plan_destroy(p->edge[k]);
+    p->edge[0] = p->edge[1] = nullptr;
+    p->nedge = 0;
+    g_last_error.clear();
+  }
 }
 
 extern "C" {
@@ -192,12 +312,14 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
     ttcb_plan_destroy(p);  // frees whatever the device set-up created
     return s;
   }
+  plan_create_edges(p);
   *plan = p;
   return TTCB_OK;
 }
 
 void ttcb_plan_destroy(ttcb_plan* plan) {
   if (!plan) return;
+  for (int k = 0; k < plan->nedge; ++k) ttcb_plan_destroy(plan->edge[k]);
   if (plan->dev_desc) cudaFree(plan->dev_desc);
   if (plan->side_stream) cudaStreamDestroy(static_cast<cudaStream_t>(plan->side_stream));
   if (plan->ev_fork) cudaEventDestroy(static_cast<cudaEvent_t>(plan->ev_fork));
@@ -222,55 +344,7 @@ ttcb_status ttcb_transpose(const ttcb_plan* p, const void* A, void* B, const voi
   if (dev != p->device)
     return fail(TTCB_ERR_INVALID_ARG, "plan was created on device " + std::to_string(p->device) +
                                           " but the current device is " + std::to_string(dev));
-  int va = p->vecA, vb = p->vecB;
-  while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
-  while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
-  if (p->kernel == TTCB_KERNEL_ROW) va = vb = std::min(va, vb);
-  int kernel = p->kernel, blocks = p->blocks, smem = p->smem_bytes;
-  if (kernel == TTCB_KERNEL_TILE) {
-    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
-    const int want = p->tuning.tile_variant;
-    const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
-    if ((want == 0 || want == 3) && td->async_ok) {
-      kernel = (fast_ok && td->reg_ok) ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;
-      blocks = p->blocks_async;
-      smem = p->smem_async;
-    } else if ((want == 0 || want == 2) && fast_ok) {
-      kernel = TTCB_KERNEL_TILE_FAST;
-      blocks = p->blocks_fast;
-      smem = p->smem_fast;
-    }
-  }
-  ttcb::KernelRef k = ttcb::pick_kernel(p->ta, p->tb, kernel, va, vb, variant_of(p));
-  if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (needs_large_smem(smem)) allow_large_smem(k.func);
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
-  const bool ragged = (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG) &&
-                      td->nrag0 + td->nrag1 > 0;
-  if (!ragged) {
-    e = k.fn(p, A, B, alpha, beta, st, blocks);
-    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-    return TTCB_OK;
-  }
-  // The staged kernel moves complete tiles only; the ragged-tile kernel moves the rest, on a side
-  // stream forked from the caller's stream before the staged kernel and joined back after both, so
-  // it runs beside the staged kernel (they write disjoint parts of B) instead of after it.
-  ttcb::KernelRef kr = ttcb::pick_kernel(p->ta, p->tb, TTCB_KERNEL_TILE_RAGGED, 1, 1, variant_of(p));
-  if (!kr.fn) return fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
-  if (needs_large_smem(p->smem_ragged)) allow_large_smem(kr.func);
-  cudaStream_t side = static_cast<cudaStream_t>(p->side_stream);
-  cudaEvent_t fork = static_cast<cudaEvent_t>(p->ev_fork), join = static_cast<cudaEvent_t>(p->ev_join);
-  std::lock_guard<std::mutex> lk(*static_cast<std::mutex*>(p->fork_mutex));
-  if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
-  if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
-  e = k.fn(p, A, B, alpha, beta, st, blocks);
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  e = kr.fn(p, A, B, alpha, beta, side, p->blocks_ragged);
-  if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
-  if ((e = cudaEventRecord(join, side)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
-  if ((e = cudaStreamWaitEvent(st, join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
-  return TTCB_OK;
+  return launch_plan(p, A, B, alpha, beta, reinterpret_cast<cudaStream_t>(stream));
 }
 
 size_t ttcb_plan_describe(const ttcb_plan* plan, char* buf, size_t len) {
@@ -421,6 +495,54 @@ size_t ttcb_test_plan_host_desc(int rank, const int* perm, const int64_t* size, 
   if (kernel) *kernel = p.kernel;
   if (buf && len >= p.host_desc.size()) std::memcpy(buf, p.host_desc.data(), p.host_desc.size());
   return p.host_desc.size();
+}
+
+size_t ttcb_test_plan_edges(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                            int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len) {
+  ttcb_plan p;
+  if (rank < 1 || rank > TTCB_MAX_RANK) return 0;
+  p.rank = rank;
+  for (int i = 0; i < rank; ++i) {
+    p.perm[i] = perm[i];
+    p.size[i] = size[i];
+  }
+  for (int j = 0; j < rank; ++j)
+    if (perm[j] < 0 || perm[j] >= rank) return 0;
+  for (int i = 0; i < rank; ++i) p.lda[i] = lda ? lda[i] : size[i];
+  for (int j = 0; j < rank; ++j) p.ldb[j] = ldb ? ldb[j] : size[perm[j]];
+  p.ta = (ttcb_dtype)type_a;
+  p.tb = (ttcb_dtype)type_b;
+  p.beta_nonzero = beta_nonzero;
+  if (tuning) p.tuning = *tuning;
+  std::string err;
+  if (plan_build_host(&p, err) != TTCB_OK) {
+    g_last_error = err;
+    return 0;
+  }
+  EdgeBox box[2];
+  const int n = p.kernel == TTCB_KERNEL_TILE ? plan_edge_boxes(&p, box) : 0;
+  std::ostringstream o;
+  o << "[";
+  for (int k = 0; k < n; ++k) {
+    const EdgeBox& b = box[k];
+    o << (k ? "," : "") << "{\"rank\":" << b.rank;
+    const char* names[] = {"perm", "size", "lda", "ldb"};
+    for (int a = 0; a < 4; ++a) {
+      o << ",\"" << names[a] << "\":[";
+      for (int i = 0; i < b.rank; ++i)
+        o << (i ? "," : "") << (a == 0 ? (int64_t)b.perm[i] : a == 1 ? b.size[i] : a == 2 ? b.lda[i] : b.ldb[i]);
+      o << "]";
+    }
+    o << ",\"offA\":" << b.offA << ",\"offB\":" << b.offB << "}";
+  }
+  o << "]";
+  const std::string js = o.str();
+  if (buf && len) {
+    size_t m = std::min(len - 1, js.size());
+    std::memcpy(buf, js.data(), m);
+    buf[m] = 0;
+  }
+  return js.size() + 1;
 }
 
 // Layout of the descriptor structs, so host-side checkers can parse them.

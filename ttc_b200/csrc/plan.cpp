@@ -147,6 +147,11 @@ static int64_t run_len(const std::vector<int>& order, const int64_t* ext, const 
 #ifndef TTCB_RAGGED_COST
 #define TTCB_RAGGED_COST 1.5
 #endif
+// Cost factor of a tile that the register-offset path cannot hold (more than 1024 vectors on a
+// side), which then reads its element offsets from shared-memory tables.
+#ifndef TTCB_TABLE_PATH_COST
+#define TTCB_TABLE_PATH_COST 1.6
+#endif
 
 static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const ttcb_tuning& tu, TileCand& c) {
   std::vector<int> aord, bord;
@@ -185,6 +190,8 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
       gA = gcd64(gA, e * f.sA[d]);
       gB = gcd64(gB, e * f.sB[d]);
     }
+    gA = gcd64(gA, f.oA);
+    gB = gcd64(gB, f.oB);
   }
   c.galA = gA;
   c.galB = gB;
@@ -212,7 +219,7 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   per_elem += 0.6 * EB * (16.0 / (c.vecB * EB) - 1.0) / 15.0 * 4.0 * (beta ? 1.5 : 1.0);
   // the fast kernel keeps at most 4 vectors per thread and phase
   const bool fast = (c.P / c.vecA <= 1024) && (c.P / c.vecB <= 1024);
-  if (!fast) per_elem *= 1.6;
+  if (!fast) per_elem *= TTCB_TABLE_PATH_COST;
 
   // average useful elements per tile (ragged last blocks waste a tile's fixed cost)
   double fill = 1.0;
@@ -575,10 +582,12 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   }
   int ng = 0, nb = 0;
   int64_t ntiles = 1;
+  int gdim_of[TTCB_MAXR];  // fused dimension of each grid dimension
   for (int d : gdims) {
     if (c.ext[d] > 0 && c.ext[d] == f.n[d]) continue;
     int64_t e = c.ext[d] > 0 ? c.ext[d] : 1;
     int64_t cnt = (f.n[d] + e - 1) / e;
+    gdim_of[ng] = d;
     GridDimDesc& g = td.g[ng++];
     g.div = make_fastdiv((uint32_t)cnt);
     g.divf = make_fastdiv((uint32_t)(c.ext[d] > 0 && f.n[d] % e != 0 ? cnt - 1 : cnt));
@@ -607,6 +616,14 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       else
         td.rag_b = k;
     }
+  p->rag_dim[0] = p->rag_dim[1] = -1;
+  p->rag_start[0] = p->rag_start[1] = 0;
+  for (int k = 0; k < 2; ++k) {
+    const int gk = k == 0 ? td.rag_a : td.rag_b;
+    if (gk < 0) continue;
+    p->rag_dim[k] = gdim_of[gk];
+    p->rag_start[k] = (int64_t)(td.g[gk].div.d - 1) * td.g[gk].e;
+  }
   {
     const int64_t ca = td.rag_a >= 0 ? td.g[td.rag_a].div.d : 1, cb = td.rag_b >= 0 ? td.g[td.rag_b].div.d : 1;
     td.nrag0 = td.rag_a >= 0 ? (int32_t)(ntiles / ca) : 0;
@@ -679,6 +696,7 @@ static ttcb_status build_row_desc(ttcb_plan* p, std::string& err) {
     g = gcd64(g, f.sA[i]);
     g = gcd64(g, f.sB[i]);
   }
+  g = gcd64(gcd64(g, f.oA), f.oB);
   int V = 16 / std::max(EA, EB);
   while (V > 1 && !(g == 0 || g % V == 0)) V /= 2;
   if (p->tuning.vec == 1) V = 1;
@@ -788,6 +806,8 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
     return TTCB_OK;
   }
   fuse_problem(r, p->perm, p->size, sA, sB, p->f);
+  p->f.oA = p->base_offA;
+  p->f.oB = p->base_offB;
   const FusedProblem& f = p->f;
   for (int i = 0; i < f.rank; ++i)
     if (f.n[i] >= (int64_t(1) << 31) && !(f.perm[0] == 0 && i == 0)) {
@@ -860,6 +880,55 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
 }
 
 // ------------------------------------------------------------------------------------------------
+// The ragged tiles of a tile plan cover the last block [start, n) of each ragged fused dimension:
+// box 0 is that block of the first ragged dimension with every other dimension whole; box 1 is the
+// last block of the second one with the first dimension below its start. Each box keeps the fused
+// strides, written as TTC leading dimensions: consecutive fused strides divide each other (they are
+// products of the caller's leading dimensions), and a unit dimension in front carries a first
+// stride other than 1.
+int plan_edge_boxes(const ttcb_plan* p, EdgeBox out[2]) {
+  const FusedProblem& f = p->f;
+  int n = 0;
+  while (n < 2 && p->rag_dim[n] >= 0) ++n;
+  if (n == 0) return 0;
+  const int r = f.rank;
+  const int s = (f.sA[0] != 1 || f.sB[f.perm[0]] != 1) ? 1 : 0;
+  if (r + s > TTCB_MAXR) return -1;
+  for (int k = 0; k < n; ++k) {
+    int64_t lo[TTCB_MAXR], ext[TTCB_MAXR];
+    for (int i = 0; i < r; ++i) {
+      lo[i] = 0;
+      ext[i] = f.n[i];
+    }
+    const int d = p->rag_dim[k];
+    lo[d] = p->rag_start[k];
+    ext[d] = f.n[d] - p->rag_start[k];
+    if (k == 1) ext[p->rag_dim[0]] = p->rag_start[0];
+    EdgeBox& b = out[k];
+    b.offA = b.offB = 0;
+    for (int i = 0; i < r; ++i) {
+      b.offA += lo[i] * f.sA[i];
+      b.offB += lo[i] * f.sB[i];
+    }
+    b.rank = r + s;
+    if (s) {
+      b.perm[0] = 0;
+      b.size[0] = 1;
+      b.lda[0] = f.sA[0];
+      b.ldb[0] = f.sB[f.perm[0]];
+    }
+    for (int i = 0; i < r; ++i) {
+      b.size[i + s] = ext[i];
+      b.lda[i + s] = i + 1 < r ? f.sA[i + 1] / f.sA[i] : ext[i];
+    }
+    for (int j = 0; j < r; ++j) {
+      b.perm[j + s] = f.perm[j] + s;
+      b.ldb[j + s] = j + 1 < r ? f.sB[f.perm[j + 1]] / f.sB[f.perm[j]] : ext[f.perm[j]];
+    }
+  }
+  return n;
+}
+
 std::string plan_describe_json(const ttcb_plan* p) {
   static const char* names[] = {"s", "d", "c", "z"};
   std::ostringstream o;
@@ -877,6 +946,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
   o << ",\"kernel\":\"" << (p->kernel == TTCB_KERNEL_TILE ? "tile" : p->kernel == TTCB_KERNEL_ROW ? "row" : "none")
     << "\",\"vecA\":" << p->vecA << ",\"vecB\":" << p->vecB << ",\"blocks\":" << p->blocks
     << ",\"streaming\":" << (p->streaming ? 1 : 0) << ",\"loop_order\":" << p->loop_order
+    << ",\"tile_variant\":" << p->tuning.tile_variant
     << ",\"smem\":" << p->smem_bytes << ",\"est_cost\":" << p->est_cost;
   if (p->kernel == TTCB_KERNEL_TILE && !p->host_desc.empty()) {
     const TileDesc* t = reinterpret_cast<const TileDesc*>(p->host_desc.data());
@@ -896,6 +966,13 @@ std::string plan_describe_json(const ttcb_plan* p) {
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {
     const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
     o << ",\"row\":{\"w\":" << rd->w << ",\"chunk\":" << rd->chunk << ",\"units\":" << rd->nunits << "}";
+  }
+  if (p->nedge > 0) {
+    o << ",\"edges\":[";
+    for (int k = 0; k < p->nedge; ++k)
+      o << (k ? "," : "") << "{\"offA\":" << p->edge[k]->base_offA << ",\"offB\":" << p->edge[k]->base_offB
+        << ",\"plan\":" << plan_describe_json(p->edge[k]) << "}";
+    o << "]";
   }
   o << "}";
   return o.str();

@@ -12,6 +12,20 @@ struct FusedProblem {
   int64_t n[TTCB_MAXR] = {0};    // extents (A order)
   int64_t sA[TTCB_MAXR] = {0};   // A stride of A-dim i
   int64_t sB[TTCB_MAXR] = {0};   // B stride of A-dim i
+  int64_t oA = 0, oB = 0;        // offsets (elements) of A and B from a 16-byte boundary; only their
+                                 // alignment matters (nonzero for the edge plans of another plan)
+};
+
+// A box of a tile plan's ragged tiles (the last block of one ragged dimension; with two ragged
+// dimensions, the second box leaves out the first's), as a transposition of its own in TTC's form:
+// the parent's strides through lda/ldb, its first element at offA / offB.
+struct EdgeBox {
+  int rank = 0;
+  int perm[TTCB_MAXR] = {0};
+  int64_t size[TTCB_MAXR] = {0};
+  int64_t lda[TTCB_MAXR] = {0};
+  int64_t ldb[TTCB_MAXR] = {0};
+  int64_t offA = 0, offB = 0;
 };
 
 struct ttcb_plan {
@@ -56,6 +70,16 @@ struct ttcb_plan {
   int smem_ragged = 0;    // its dynamic shared memory (two tile buffers + tables)
   int device = 0;
 
+  // ragged tiles: the fused dimensions whose last tile block is ragged and where that block starts
+  int rag_dim[2] = {-1, -1};
+  int64_t rag_start[2] = {0, 0};
+  // edge plans: the boxes of the ragged tiles planned as transpositions of their own, which the
+  // staged kernel moves on the side stream (instead of the element-wise ragged-tile kernel)
+  int depth = 0;                     // 0 for a caller's plan, 1 for an edge plan
+  int64_t base_offA = 0, base_offB = 0;  // an edge plan's offsets into its parent's A and B
+  ttcb_plan* edge[2] = {nullptr, nullptr};
+  int nedge = 0;
+
   // shape-only planning (candidate features for the learned selector): the tile choice without
   // descriptor tables
   bool shape_only = false;
@@ -76,6 +100,10 @@ void plan_tile_cache_end();
 // the test helper in abi.cu).
 void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA, const int64_t* sB,
                   FusedProblem& out);
+
+// The boxes of a tile plan's ragged tiles (0, 1 or 2); -1 when they cannot be written in TTC's form
+// within the rank limit.
+int plan_edge_boxes(const ttcb_plan* p, EdgeBox out[2]);
 
 int dtype_bytes(ttcb_dtype t);
 std::string plan_describe_json(const ttcb_plan* p);

@@ -22,4 +22,8 @@ void ttcb_test_desc_layout(int64_t* out);
 size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
                              int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tunings, int n, char* buf,
                              size_t len);
+// The boxes a plan's ragged tiles are moved as (edge plans), host-only: a JSON array of
+// {"rank","perm","size","lda","ldb","offA","offB"}; returns the length needed, 0 on failure.
+size_t ttcb_test_plan_edges(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
+                            int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len);
 }
