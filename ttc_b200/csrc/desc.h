@@ -56,7 +56,7 @@ struct TileDesc {
   int32_t async_ok;   // 1: the staged kernel applies (32-bit offsets, <= 16 elements per thread)
   int32_t padA;       // padding after each A run in the staged layout (multiple of the A vector)
   int32_t stage_elems;// elements of one stage buffer (max of the staged layout and phys_size)
-  int32_t nstages;    // staged kernel: stages (3 or 4; stages - 2 tiles of copies in flight)
+  int32_t nstages;    // staged kernel: stages (3..7; stages - 2 tiles of copies in flight)
   int32_t off_gtab;   // byte offset of gtab (uint16_t[P]) from the start of the descriptor
   int32_t sigmaA;     // staged layout: element p at p + (p / sigmaA) * padA
   int32_t reg_ok;     // 1: fast, and the staged tile's byte offsets fit 16 bits (register path)

@@ -490,9 +490,11 @@ __host__ __device__ inline size_t async_smem_bytes(int S, int stage_elems, int P
          (P > kRegPos * kThreads ? al16((size_t)2 * P) : 0);
 }
 
-// Decoded tile, shared by the CTA: thread 0 decodes each tile once, S iterations ahead, into a
-// four-entry ring (tile j of this CTA in entry j & 3). The entry written in iteration k is read
-// only after that iteration's barriers, and its previous tile was consumed before them.
+// Decoded tile, shared by the CTA: thread 0 decodes each tile once, D + 2 iterations ahead (D = S - 2
+// tiles of copies in flight), into a ring of kInfoRing entries (tile j of this CTA in entry
+// j % kInfoRing). Iteration k reads entries k .. k + D + 1 and writes entry k + D + 2 after its
+// barrier, whose previous tile (k + D + 2 - kInfoRing <= k - 1 for S <= kMaxStages) every thread
+// finished with before that barrier.
 struct TileInfo {
   int64_t bA, bB;
   int32_t state;  // 1: complete tile, 0: ragged tile, -1: past the last tile
@@ -502,6 +504,8 @@ struct TileInfo {
 // Static shared memory of the staged kernel (descriptor header + tile ring), on top of its dynamic
 // shared memory.
 constexpr int kInfoRing = 8;  // staged kernel: decoded-tile ring entries (tile j in entry j % 8)
+constexpr int kMaxStages = kInfoRing - 1;  // D + 3 <= kInfoRing ring entries live at once
+static_assert(kMaxStages - 2 <= 5, "the copy-group wait covers at most 5 tiles in flight");
 constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileInfo);
 
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
@@ -509,7 +513,7 @@ constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileIn
 // source offsets rA, staged byte offsets dA (two per register), B offsets rB, gather byte offsets
 // gp (two per register; B vector u = tid + u * kThreads, element j). Otherwise offsets are computed
 // per vector from the run tables in shared memory, with the gather positions in registers while
-// P <= kRegPos * kThreads and in shared memory beyond. The number of stages (3 or 4) is the
+// P <= kRegPos * kThreads and in shared memory beyond. The number of stages (3 to kMaxStages) is the
 // descriptor's.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG>
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
@@ -683,10 +687,14 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     if (t >= ntiles) break;
     issue(info[(k + D) % kInfoRing], nxt);
     cp_async_commit();
-    if (D == 2)
-      cp_async_wait<2>();
-    else
-      cp_async_wait<1>();
+    // tile k's copies are complete once at most D groups (tiles k + 1 .. k + D) are pending
+    switch (D) {
+      case 1: cp_async_wait<1>(); break;
+      case 2: cp_async_wait<2>(); break;
+      case 3: cp_async_wait<3>(); break;
+      case 4: cp_async_wait<4>(); break;
+      default: cp_async_wait<5>(); break;
+    }
     __syncthreads();
     if (tid == 0) decode_into(t + (D + 2) * G, info[(k + D + 2) % kInfoRing]);
     const TileInfo& ti = info[k % kInfoRing];

@@ -661,7 +661,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       return (int64_t)ttcb::async_smem_bytes(S, td.stage_elems, (int)P, (int)nsegA, (int)nsegB, EA, EB, beta);
     };
     // four stages (two tiles of copies in flight) while four CTAs still fit an SM (about 56 KB
-    // each), else three (one tile in flight)
+    // each), else three (one tile in flight); deeper rings (up to ttcb::kMaxStages) measured
+    // slower on the sweep, with four CTAs or with fewer
     td.nstages = smem_for(4) <= 56 * 1024 ? 4 : 3;
     td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
