@@ -364,6 +364,24 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
 
 
 # ------------------------------------------------------------------------------------------------
+def fallback_set(order: np.ndarray, default: int, topk: int) -> list:
+    """Candidates a low-confidence selection times: the network's best topk - 1 and the planner's
+    default schedule (its top topk when the default is among them), so that a doubtful prediction
+    is checked against the method without the network."""
+    head = [int(i) for i in order[: max(topk - 1, 1)]]
+    if default in head or default < 0:
+        return [int(i) for i in order[:topk]]
+    return head + [int(default)]
+
+
+def default_index(tunings: list) -> int:
+    """Position of the planner's default schedule (the empty tuning) among candidate tunings."""
+    for i, tu in enumerate(tunings):
+        if not tu:
+            return i
+    return -1
+
+
 def confidence_of(pred: np.ndarray, rmse: float) -> float:
     """1 - exp(-gap / rmse): gap = predicted log-GB/s margin of the best over the second-best."""
     if len(pred) < 2:
@@ -384,8 +402,9 @@ def load_default(path: Optional[Path] = None) -> MLP:
 
 def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, verify: bool = True,
            model: Optional[MLP] = None, topk: int = 2, measure_choice: bool = True) -> dict:
-    """Picks a schedule with the model. Below the confidence threshold, measures the top-k
-    predictions and keeps the fastest (a short measured search). Returns the measured results."""
+    """Picks a schedule with the model. Below the confidence threshold, measures the network's
+    top-(k-1) predictions and the planner's default schedule and keeps the fastest (a short
+    measured search). Returns the measured results."""
     model = model or load_default()
     thr = 0.1 if confidence is None else confidence
     t0 = time.perf_counter()
@@ -395,7 +414,8 @@ def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, v
     order = np.argsort(-pred)
     conf = confidence_of(pred, model.rmse)
     fallback = conf < thr
-    chosen = [cands[i][0] for i in order[: (topk if fallback else 1)]]
+    picks = fallback_set(order, default_index([c[0] for c in cands]), topk) if fallback else [int(order[0])]
+    chosen = [cands[i][0] for i in picks]
     t_model = time.perf_counter() - t0
     results = measure(p, chosen, reps=3, verify=verify) if (measure_choice or fallback) else []
     return {"results": results, "confidence": conf, "fallback": fallback, "pred": pred, "order": order,
@@ -461,8 +481,8 @@ def _save_corpus(out: Path, d: dict):
 def stored_selection(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: dict, rmse: float,
                      threshold: float, topk: int) -> dict:
     """Selection quality on stored exhaustive measurements: per problem, the GB/s of the model's
-    top-1 (or best of its top-k when its confidence is below the threshold) and of the planner's
-    default schedule, over the best measured GB/s."""
+    top-1 (or, when its confidence is below the threshold, the best of the timed fallback set: its
+    top-(k-1) and the default) and of the planner's default schedule, over the best measured GB/s."""
     index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
     top1, gated, dflt, fb = [], [], [], []
     for k in np.unique(case):
@@ -473,8 +493,8 @@ def stored_selection(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: di
         top1.append(np.exp(y[rows[order[0]]] - best))
         low = confidence_of(pred[rows], rmse) < threshold
         fb.append(low)
-        gated.append(np.exp(y[rows[order[:topk]]].max() - best) if low else top1[-1])
         d = tunings.index({}) if {} in tunings else 0
+        gated.append(np.exp(y[rows[fallback_set(order, d, topk)]].max() - best) if low else top1[-1])
         dflt.append(np.exp(y[rows[d]] - best))
     top1, gated, dflt = map(np.asarray, (top1, gated, dflt))
     return {"cases": int(len(top1)), "top1_over_best": float(top1.mean()),
