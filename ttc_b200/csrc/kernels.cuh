@@ -490,11 +490,13 @@ __host__ __device__ inline size_t async_smem_bytes(int S, int stage_elems, int P
          (P > kRegPos * kThreads ? al16((size_t)2 * P) : 0);
 }
 
-// Decoded tile, shared by the CTA: thread 0 decodes each tile once, D + 2 iterations ahead (D = S - 2
-// tiles of copies in flight), into a ring of kInfoRing entries (tile j of this CTA in entry
-// j % kInfoRing). Iteration k reads entries k .. k + D + 1 and writes entry k + D + 2 after its
-// barrier, whose previous tile (k + D + 2 - kInfoRing <= k - 1 for S <= kMaxStages) every thread
-// finished with before that barrier.
+// Decoded tile, shared by the CTA. The first kDecodeBatch lanes of warp 0 decode tiles in batches:
+// before the loop, tiles 0 .. 2 * kDecodeBatch - 1 of this CTA; after the barrier of iteration k (k a
+// nonzero multiple of kDecodeBatch), tiles k + kDecodeBatch .. k + 2 * kDecodeBatch - 1, one per lane,
+// into the ring entries (j % kInfoRing) of tiles k - kDecodeBatch .. k - 1, which every thread
+// finished with before that barrier. Tile k + D, issued in iteration k, was decoded at the latest in
+// iteration k - kDecodeBatch (D < kDecodeBatch), so one lane's decode costs warp 0 an eighth of a
+// tile decode per iteration instead of a whole one.
 struct TileInfo {
   int64_t bA, bB;
   int32_t state;  // 1: complete tile, 0: ragged tile, -1: past the last tile
@@ -503,9 +505,11 @@ struct TileInfo {
 
 // Static shared memory of the staged kernel (descriptor header + tile ring), on top of its dynamic
 // shared memory.
-constexpr int kInfoRing = 8;  // staged kernel: decoded-tile ring entries (tile j in entry j % 8)
-constexpr int kMaxStages = kInfoRing - 1;  // D + 3 <= kInfoRing ring entries live at once
-static_assert(kMaxStages - 2 <= 5, "the copy-group wait covers at most 5 tiles in flight");
+constexpr int kDecodeBatch = 8;              // staged kernel: tiles decoded per batch
+constexpr int kInfoRing = 2 * kDecodeBatch;  // decoded-tile ring entries (tile j in entry j % kInfoRing)
+constexpr int kMaxStages = 7;                // S - 2 = D tiles in flight, D < kDecodeBatch
+static_assert(kMaxStages - 2 < kDecodeBatch && kMaxStages - 2 <= 5,
+              "tiles in flight must be decoded a batch ahead and covered by the copy-group wait");
 constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileInfo);
 
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
@@ -668,11 +672,10 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
 
   // Pipeline: S stages, D = S - 2 tiles of copies in flight ahead of the tile being written, and one
   // CTA barrier per tile. Iteration k issues tile k + D into stage (k + D) % S, whose previous tile
-  // (k - 2) every thread finished writing out before the barrier of iteration k - 1; thread 0
-  // decodes tile k + D + 2, which iteration k + 2 issues after the barrier of iteration k + 1.
+  // (k - 2) every thread finished writing out before the barrier of iteration k - 1. Tiles are
+  // decoded in batches (see TileInfo).
   const int D = S - 2;
-  if (tid == 0)
-    for (int j = 0; j < D + 2; ++j) decode_into(blockIdx.x + j * G, info[j]);
+  if (tid < kInfoRing) decode_into(blockIdx.x + tid * G, info[tid]);
   __syncthreads();
   // everything above reads the plan's descriptor only; A and B are touched from here on
   pdl_wait_previous();
@@ -696,7 +699,8 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       default: cp_async_wait<5>(); break;
     }
     __syncthreads();
-    if (tid == 0) decode_into(t + (D + 2) * G, info[(k + D + 2) % kInfoRing]);
+    if (tid < kDecodeBatch && k % kDecodeBatch == 0 && k != 0)
+      decode_into(t + (kDecodeBatch + tid) * G, info[(k + kDecodeBatch + tid) % kInfoRing]);
     const TileInfo& ti = info[k % kInfoRing];
     TB* Bt = B + ti.bB;
     const unsigned char* stage = smem_raw + cur * sbytes;
