@@ -15,7 +15,8 @@ struct BatchProblem {
   const unsigned char* desc;  // TileDesc or RowDesc, followed by its tables (device memory)
   int32_t kind;               // TTCB_KERNEL_TILE / TTCB_KERNEL_ROW
   int32_t va, vb;             // access widths for this problem (1 = scalar)
-  int32_t pad_;
+  int32_t full_only;          // tile problem: items are its complete tiles only (edge plans, problems
+                              // of their own, move its ragged tiles)
 };
 
 // Stage buffers of the batched kernel's tile pipeline (tiles in flight ahead of the one written out:
@@ -220,7 +221,11 @@ __global__ void __launch_bounds__(kThreads, 3) batch_kernel(const BatchProblem* 
       }
       int64_t bA, bB;
       int lim[2];
-      const bool full = decode_tile(d, local, bA, bB, lim);
+      bool full = true;
+      if (bp->full_only)
+        decode_full_tile(d, local, bA, bB);
+      else
+        full = decode_tile(d, local, bA, bB, lim);
       const TA* A = static_cast<const TA*>(bp->A);
       if (full) {
         // the buffer after the newest pending one is free: its previous tile was written out

@@ -109,9 +109,18 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
   std::memcpy(b->alpha, alpha, EA);
   if (p0->beta_nonzero) std::memcpy(b->beta, beta, EB);
 
-  // descriptors back to back, 16-byte aligned
-  std::vector<int64_t> desc_off(count, -1);
-  int64_t desc_bytes = 0;
+  // Problems of the batch: every plan, and for a plan whose ragged tiles its edge plans move, those
+  // edge plans as problems of their own (offset into the plan's A and B) while the plan keeps only
+  // its complete tiles.
+  struct Entry {
+    const ttcb_plan* p;
+    const void* A;
+    void* B;
+    int full_only;  // the plan's complete tiles only (its edge plans follow it)
+    int user;       // index of the caller's plan
+  };
+  std::vector<Entry> ent;
+  ent.reserve(count);
   for (int i = 0; i < count; ++i) {
     const ttcb_plan* p = plans[i];
     if (!p) {
@@ -126,68 +135,84 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
       batch_free(b);
       return bfail(TTCB_ERR_INVALID_ARG, "plan " + std::to_string(i) + " belongs to another device");
     }
-    if (!p->empty) {
+    if (!p->empty && (!A[i] || !B[i])) {
+      batch_free(b);
+      return bfail(TTCB_ERR_INVALID_ARG, "A or B of problem " + std::to_string(i) + " is NULL");
+    }
+    const bool edges = !p->empty && p->kernel == TTCB_KERNEL_TILE && p->nedge > 0;
+    ent.push_back({p, A[i], B[i], edges ? 1 : 0, i});
+    for (int k = 0; edges && k < p->nedge; ++k) {
+      const ttcb_plan* q = p->edge[k];
+      ent.push_back({q, static_cast<const char*>(A[i]) + q->base_offA * EA,
+                     static_cast<char*>(B[i]) + q->base_offB * EB, 0, i});
+    }
+  }
+  const int n = (int)ent.size();
+  b->count = n;
+
+  // descriptors back to back, 16-byte aligned
+  std::vector<int64_t> desc_off(n, -1);
+  int64_t desc_bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!ent[i].p->empty) {
       desc_off[i] = desc_bytes;
-      desc_bytes += (p->host_desc.size() + 15) & ~size_t(15);
+      desc_bytes += (ent[i].p->host_desc.size() + 15) & ~size_t(15);
     }
   }
   std::vector<unsigned char> hdesc(std::max<int64_t>(desc_bytes, 16), 0);
-  std::vector<ttcb::BatchProblem> hp(count);
-  std::vector<int64_t> prefix(count + 1, 0);
+  std::vector<ttcb::BatchProblem> hp(n);
+  std::vector<int64_t> prefix(n + 1, 0);
   int max_slots_bytes = 0, max_table_bytes = 0;
-  for (int i = 0; i < count; ++i) {
-    const ttcb_plan* p = plans[i];
+  for (int i = 0; i < n; ++i) {
+    const ttcb_plan* p = ent[i].p;
     ttcb::BatchProblem& q = hp[i];
     std::memset(&q, 0, sizeof(q));
     int64_t items = 0;
     if (!p->empty) {
-      if (!A[i] || !B[i]) {
-        batch_free(b);
-        return bfail(TTCB_ERR_INVALID_ARG, "A or B of problem " + std::to_string(i) + " is NULL");
-      }
       std::memcpy(hdesc.data() + desc_off[i], p->host_desc.data(), p->host_desc.size());
-      q.A = A[i];
-      q.B = B[i];
+      q.A = ent[i].A;
+      q.B = ent[i].B;
       q.kind = p->kernel;
       q.va = p->vecA;
       q.vb = p->vecB;
-      while (q.va > 1 && (uintptr_t)A[i] % (q.va * EA)) q.va /= 2;
-      while (q.vb > 1 && (uintptr_t)B[i] % (q.vb * EB)) q.vb /= 2;
+      q.full_only = ent[i].full_only;
+      while (q.va > 1 && (uintptr_t)q.A % (q.va * EA)) q.va /= 2;
+      while (q.vb > 1 && (uintptr_t)q.B % (q.vb * EB)) q.vb /= 2;
       if (p->kernel == TTCB_KERNEL_ROW) {
         q.va = q.vb = std::min(q.va, q.vb);
         const RowDesc* rd = reinterpret_cast<const RowDesc*>(p->host_desc.data());
         items = (rd->nunits + 7) / 8;
       } else {
         const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
-        items = td->ntiles;
+        items = ent[i].full_only ? td->nfull : td->ntiles;
         // one stage buffer: the staged layout (or, for a ragged tile, the slots), 16-byte aligned
         max_slots_bytes = std::max<int>(
             max_slots_bytes, (int)ttcb::al16((size_t)std::max(td->stage_elems, td->phys_size) * EA));
         max_table_bytes = std::max<int>(max_table_bytes, 8 * (td->nsegA + td->nsegB) + 4 * ((td->P + 1) / 2));
       }
-      b->bytes += ttcb_plan_bytes(p);
+      if (p == plans[ent[i].user]) b->bytes += ttcb_plan_bytes(p);  // an edge plan's bytes are its parent's
     }
     prefix[i + 1] = prefix[i] + items;
   }
-  b->total = (unsigned long long)prefix[count];
+  b->total = (unsigned long long)prefix[n];
   b->slots_bytes = (int)((max_slots_bytes + 15) & ~15);
   b->smem = ttcb::kBatchStages * b->slots_bytes + max_table_bytes;  // stage buffers, then the tables
 
   // device copies
   if ((e = cudaMalloc(&b->d_desc, hdesc.size())) != cudaSuccess ||
-      (e = cudaMalloc(&b->d_probs, sizeof(ttcb::BatchProblem) * count)) != cudaSuccess ||
-      (e = cudaMalloc(&b->d_prefix, sizeof(int64_t) * (count + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&b->d_probs, sizeof(ttcb::BatchProblem) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&b->d_prefix, sizeof(int64_t) * (n + 1))) != cudaSuccess ||
       (e = cudaMalloc(&b->d_counter, 2 * sizeof(unsigned long long))) != cudaSuccess) {
     cudaGetLastError();
     batch_free(b);
     return bfail(TTCB_ERR_ALLOC, std::string("cudaMalloc for the batch failed: ") + cudaGetErrorString(e));
   }
-  for (int i = 0; i < count; ++i)
+  for (int i = 0; i < n; ++i)
     if (desc_off[i] >= 0) hp[i].desc = b->d_desc + desc_off[i];
   if ((e = cudaMemcpy(b->d_desc, hdesc.data(), hdesc.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-      (e = cudaMemcpy(b->d_probs, hp.data(), sizeof(ttcb::BatchProblem) * count, cudaMemcpyHostToDevice)) !=
+      (e = cudaMemcpy(b->d_probs, hp.data(), sizeof(ttcb::BatchProblem) * n, cudaMemcpyHostToDevice)) !=
           cudaSuccess ||
-      (e = cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice)) !=
+      (e = cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice)) !=
           cudaSuccess ||
       (e = cudaMemset(b->d_counter, 0, 2 * sizeof(unsigned long long))) != cudaSuccess) {
     batch_free(b);
