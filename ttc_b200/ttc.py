@@ -195,7 +195,7 @@ def _tunings_from_args(a: TTCargs, dtype: str):
         for lp in a.loopPermutations:
             lp = list(lp)
             if lp == sorted(lp):
-                orders.add(0)
+                orders.add(3)
             elif lp == sorted(lp, reverse=True):
                 orders.add(2)
             else:
