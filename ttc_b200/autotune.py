@@ -68,7 +68,10 @@ def knob_space(dtype: str) -> dict:
     return {
         "tile_elems": [0, base // 4, base // 2, base * 2],
         "run_bytes": [0, 128, 256, 512, 1024, 2048],
-        "tile_variant": [0, 2, 1],
+        # the register-prefetch (2) and table-driven (1) tile kernels were the fastest schedule for 12
+        # of the 2000 timed training problems (none by more than noise on the 500 held out) while
+        # taking a fifth of the candidates, so the search leaves them to explicit schedules
+        "tile_variant": [0],
         "loop_order": [0, 1, 2, 3],
         "blocks": [0, 2 * SMS, 3 * SMS],
     }

@@ -206,22 +206,24 @@ static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const
   std::lock_guard<std::mutex> lk(*static_cast<std::mutex*>(p->fork_mutex));
   if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
   if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+  // once forked, the side stream is joined back even when a launch fails, so that the caller's
+  // stream stays ordered after whatever was enqueued
+  ttcb_status status = TTCB_OK;
   e = k.fn(p, A, B, alpha, beta, st, blocks);
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  if (p->nedge > 0) {
-    for (int j = 0; j < p->nedge; ++j) {
+  if (e != cudaSuccess) status = cuda_fail(e, "kernel launch");
+  if (status == TTCB_OK && p->nedge > 0) {
+    for (int j = 0; j < p->nedge && status == TTCB_OK; ++j) {
       const ttcb_plan* q = p->edge[j];
-      ttcb_status s = launch_plan(q, static_cast<const char*>(A) + q->base_offA * EA,
-                                  static_cast<char*>(B) + q->base_offB * EB, alpha, beta, side);
-      if (s != TTCB_OK) return s;
+      status = launch_plan(q, static_cast<const char*>(A) + q->base_offA * EA,
+                           static_cast<char*>(B) + q->base_offB * EB, alpha, beta, side);
     }
-  } else {
+  } else if (status == TTCB_OK) {
     e = kr.fn(p, A, B, alpha, beta, side, p->blocks_ragged);
-    if (e != cudaSuccess) return cuda_fail(e, "ragged-tile kernel launch");
+    if (e != cudaSuccess) status = cuda_fail(e, "ragged-tile kernel launch");
   }
   if ((e = cudaEventRecord(join, side)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
   if ((e = cudaStreamWaitEvent(st, join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
-  return TTCB_OK;
+  return status;
 }
 
 // Edge plans: the boxes of a staged-kernel plan's ragged tiles, each planned as a transposition of
