@@ -94,7 +94,7 @@ def test_padded_lda_ldb_and_complex_beta(dtype):
     check_case([1, 2, 0], [33, 17, 9], dtype, alpha, 0.0, ldb=[17, 12, 33])
 
 
-TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"blocks": 7}, {"tile_elems": 512},
+TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"loop_order": 3}, {"blocks": 7}, {"tile_elems": 512},
            {"tile_elems": 8192}, {"run_bytes": 128}, {"run_bytes": 2048}, {"kernel": 1}, {"streaming": -1},
            {"streaming": 1}]
 
@@ -197,6 +197,7 @@ def test_torch_permute_agrees_on_large_sweep_shapes():
     from ttc_b200 import Plan
     import ttc_b200.workloads as wl
     cases = wl.sweep_cases(seed=2024)[:6]
+    rasters, edges = set(), 0
     for c in cases:
         size, perm = c["size"], c["perm"]
         tdt = torch.float32 if c["dtype"] == "s" else torch.float64
@@ -211,8 +212,13 @@ def test_torch_permute_agrees_on_large_sweep_shapes():
         want = At.permute(*[nd - 1 - perm[j] for j in reversed(range(nd))]).contiguous().view(-1)
         torch.cuda.synchronize()
         assert torch.equal(B, want), (perm, size, p.describe())
+        d = p.describe()
+        rasters.add(d["loop_order"])
+        edges += bool(d.get("edges"))
         del A, B, At, want
         torch.cuda.empty_cache()
+    # the planner's raster choice (B-major for short B runs) and edge plans are both exercised
+    assert rasters == {1, 3} and edges > 0, (rasters, edges)
 
 
 @pytest.mark.parametrize("perm,size", [([1, 0], [46341, 46341]), ([2, 0, 1], [3, 65537, 10923])])
