@@ -379,7 +379,7 @@ def main():
     return 0
 
 
-class gpu_local_cpus:
+class GpuLocalCpus:
     """Runs its body on the CPUs of the GPU's own NUMA node (from the PCI device's `local_cpulist`),
     so that pinned host buffers allocated there are first touched, and placed, on the memory next to
     the GPU's PCIe root; the process's previous CPU set is restored afterwards. A no-op where the
@@ -421,7 +421,7 @@ def run_e2e(args, items, stream, dev, world):
     import torch
     sub = items[: max(1, min(args.e2e_cases, len(items)))]
     host = []
-    with gpu_local_cpus(dev):  # pinned buffers on the host memory next to the GPU
+    with GpuLocalCpus(dev):  # pinned buffers on the host memory next to the GPU
         for c, plan, A, B in sub:
             hA = torch.empty(A.numel(), dtype=A.dtype, pin_memory=True)
             hB = torch.empty(B.numel(), dtype=B.dtype, pin_memory=True)
