@@ -98,6 +98,18 @@ void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA
 // ------------------------------------------------------------------------------------------------
 // Cost model. Units: bytes of DRAM traffic (including wasted sector bytes) per element, plus a
 // fixed per-tile overhead expressed in the same unit.
+// Fixed cost of a tile (decode, barrier, pipeline step) in bytes-equivalent.
+#ifndef TTCB_TILE_OVERHEAD
+#define TTCB_TILE_OVERHEAD 3072.0
+#endif
+// Issue cost of accesses narrower than 16 bytes (per element, scaled by the missing width).
+#ifndef TTCB_NARROW_COST
+#define TTCB_NARROW_COST 0.6
+#endif
+// Efficiency factor of a run that is shorter than 128 bytes, at zero length (linear up to 1 at 128).
+#ifndef TTCB_SHORT_RUN_FLOOR
+#define TTCB_SHORT_RUN_FLOOR 0.75
+#endif
 static double run_eff(double run_bytes, int64_t align_bytes) {
   if (run_bytes <= 0) return 1e-3;
   int64_t a = std::max<int64_t>(4, std::min<int64_t>(align_bytes, 32));
@@ -109,7 +121,7 @@ static double run_eff(double run_bytes, int64_t align_bytes) {
   }
   sectors /= cnt;
   double eff = run_bytes / (32.0 * sectors);
-  if (run_bytes < 128) eff *= 0.75 + 0.25 * run_bytes / 128.0;  // short DRAM bursts
+  if (run_bytes < 128) eff *= TTCB_SHORT_RUN_FLOOR + (1.0 - TTCB_SHORT_RUN_FLOOR) * run_bytes / 128.0;  // short bursts
   return eff;
 }
 
@@ -215,8 +227,8 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
   double effB = run_eff((double)c.LB * EB, alB);
   double per_elem = EA / effA + (beta ? 2.0 : 1.0) * EB / effB;
   // narrower accesses cost issue slots (the kernels are close to instruction-bound)
-  per_elem += 0.6 * EA * (16.0 / (c.vecA * EA) - 1.0) / 15.0 * 4.0;
-  per_elem += 0.6 * EB * (16.0 / (c.vecB * EB) - 1.0) / 15.0 * 4.0 * (beta ? 1.5 : 1.0);
+  per_elem += TTCB_NARROW_COST * EA * (16.0 / (c.vecA * EA) - 1.0) / 15.0 * 4.0;
+  per_elem += TTCB_NARROW_COST * EB * (16.0 / (c.vecB * EB) - 1.0) / 15.0 * 4.0 * (beta ? 1.5 : 1.0);
   // the fast kernel keeps at most 4 vectors per thread and phase
   const bool fast = (c.P / c.vecA <= 1024) && (c.P / c.vecB <= 1024);
   if (!fast) per_elem *= TTCB_TABLE_PATH_COST;
@@ -233,7 +245,7 @@ static void eval_tile(const FusedProblem& f, int EA, int EB, bool beta, const tt
       fill *= (double)f.n[d] / (double)(nb * c.ext[d]);
     }
   }
-  double tile_overhead = 3072.0;  // bytes-equivalent per tile
+  double tile_overhead = TTCB_TILE_OVERHEAD;  // bytes-equivalent per tile
   double cost = per_elem + tile_overhead / (c.P * fill);
   // last blocks of blocked dimensions run the element-wise ragged path
   {
