@@ -2,6 +2,7 @@
 TTC's fuseIndices, validation errors, and a CPU replay of the kernels' index arithmetic from the
 descriptor tables against the oracle's element mapping."""
 import itertools
+import json
 import re
 from pathlib import Path
 
@@ -288,3 +289,17 @@ def test_planner_raster_choice():
     assert d["tile"]["LB"] * 8 >= 256 and d["loop_order"] == 3, d
     for lo in (1, 2, 3):
         assert plan_host_json(*big_short_b, "s", False, tuning={"loop_order": lo})["loop_order"] == lo
+
+
+def test_candidate_rasters_name_each_order_once():
+    """The search's raster candidates are the planner's choice (0) plus the two orders it did not
+    choose: for a large problem with short B runs (planner: B-major) the explicit A-major order (3)
+    is searched and B-major (1) is not repeated; for a small one the reverse."""
+    from ttc_b200.autotune import Problem, candidate_tunings
+    big = Problem([4, 2, 1, 3, 0], [39, 4, 7, 153, 314], "s", 1.0, 0.0)
+    small = Problem([4, 2, 1, 3, 0], [39, 4, 7, 15, 314], "s", 1.0, 0.0)
+    for p, chosen, other in ((big, 1, 3), (small, 3, 1)):
+        cands = candidate_tunings(p, max_impl=500, with_desc=True)
+        orders = {tu.get("loop_order", 0) for tu, d in cands if d["kernel"] == "tile" and d["loop_order"] == chosen}
+        assert chosen not in orders and other in orders and 0 in orders and 2 in orders, (orders, chosen)
+        assert len({json.dumps(tu, sort_keys=True) for tu, _ in cands}) == len(cands)
