@@ -118,6 +118,9 @@ def test_kernel_index_math_replay_matches_oracle_mapping():
     ([0, 2, 1], [11, 8, 300], None, None),
     ([4, 2, 0, 3, 1], [9, 11, 7, 13, 5], None, None),
     ([0, 1, 2], [10, 20, 30], [12, 20, 30], [10, 22, 30]),
+    # shared stride-1 rows of 512..1023 bytes go to the tile kernel
+    ([0, 3, 2, 1], [156, 5, 7, 4], None, None),
+    ([0, 2, 1], [130, 9, 11], [131, 9, 11], None),
 ])
 def test_replay_larger_shapes(perm, size, lda, ldb):
     for tuning in (None, {"vec": 1}, {"loop_order": 1}):
