@@ -379,6 +379,16 @@ def main():
     return 0
 
 
+def parse_cpulist(text: str) -> set:
+    """CPU numbers of a Linux cpulist ("0-3,8,10-11")."""
+    cpus = set()
+    for part in text.strip().split(","):
+        if part:
+            lo, _, hi = part.partition("-")
+            cpus.update(range(int(lo), int(hi or lo) + 1))
+    return cpus
+
+
 class GpuLocalCpus:
     """Runs its body on the CPUs of the GPU's own NUMA node (from the PCI device's `local_cpulist`),
     so that pinned host buffers allocated there are first touched, and placed, on the memory next to
@@ -394,10 +404,7 @@ class GpuLocalCpus:
             pr = torch.cuda.get_device_properties(self.dev)
             path = Path(f"/sys/bus/pci/devices/{pr.pci_domain_id:04x}:{pr.pci_bus_id:02x}:"
                         f"{pr.pci_device_id:02x}.0/local_cpulist")
-            cpus = set()
-            for part in path.read_text().strip().split(","):
-                lo, _, hi = part.partition("-")
-                cpus.update(range(int(lo), int(hi or lo) + 1))
+            cpus = parse_cpulist(path.read_text())
             old = os.sched_getaffinity(0)
             use = cpus & old
             if use and use != old:

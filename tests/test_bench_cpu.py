@@ -1,0 +1,30 @@
+"""Host-side helpers of the benchmark and the launch accounting (no GPU)."""
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+
+def test_parse_cpulist():
+    import bench
+    assert bench.parse_cpulist("0-3,8,10-11\n") == {0, 1, 2, 3, 8, 10, 11}
+    assert bench.parse_cpulist("5") == {5}
+    assert bench.parse_cpulist("") == set()
+
+
+def test_describe_launches_counts_edge_plans():
+    """A call launches the plan's kernel, and for a staged tile plan with ragged tiles its edge plans'
+    kernels (each with its own ragged-tile kernel when it has ragged tiles) or, without edge plans,
+    the element-wise ragged-tile kernel."""
+    from ttc_b200.core import describe_launches
+    row = {"kernel": "row"}
+    plain = {"kernel": "tile", "tile": {"async": 1, "ragged_tiles": 0}}
+    edge_ragged = {"kernel": "tile", "tile": {"async": 1, "ragged_tiles": 3}}
+    assert describe_launches(row) == 1
+    assert describe_launches(plain) == 1
+    assert describe_launches(edge_ragged) == 2  # no edge plans: the ragged-tile kernel
+    parent = {"kernel": "tile", "tile": {"async": 1, "ragged_tiles": 9},
+              "edges": [{"offA": 0, "offB": 0, "plan": plain}, {"offA": 5, "offB": 7, "plan": edge_ragged}]}
+    assert describe_launches(parent) == 1 + 1 + 2
+    legacy = dict(parent, tile_variant=1)  # the legacy kernels move ragged tiles inline
+    assert describe_launches(legacy) == 1
