@@ -3,19 +3,25 @@
 
 A step = one pass over the 64-case sweep: seeded rank-2..6 transpositions with |A| ~ 200 MiB each
 (fp32/fp64, half alpha=1/beta=0, half alpha=1.5/beta=-0.5, one extent in [7, 31]), the shapes of TTC's
-200 MiB benchmark method. Inputs stay resident in HBM for `value`; `e2e` repeats the metric through
-the public call with pinned host buffers and the host<->device copies inside the timed region.
+200 MiB benchmark method. Inputs stay resident in HBM for `value`; `e2e` repeats the metric over the
+same 64 cases through the public call with pinned host buffers and the host<->device copies inside
+the timed region, beside the PCIe bandwidth measured in the same run. The CPU baseline (TTC's own
+generated AVX code, rebuilt for this host with TTC's Makefile flags) runs the same 64 cases.
+On one GPU the line also carries the other configurations: the README shape, the strided mixed-
+precision shapes, the batched workload against per-call launches, and the learned selector against
+a fresh measured search on held-out problems.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-extras]
 
 Under torchrun every rank runs its own seeded sweep (weak scaling, no collective on the data path);
 rank 0 prints one JSON line. `--impl reference` times the reference's CPU implementation of the path
-on the host cores (TTC's generated AVX code from oracle/_ref when it was built, otherwise the C port
-of TTC's reference loop) on rank 0 only.
+on the host cores (TTC's generated AVX code from oracle/_ref, rebuilt for the host; the C port of
+TTC's reference loop where it was not built) on rank 0 only, over the same 64 cases.
 """
 from __future__ import annotations
 
 import argparse
+import concurrent.futures as cf
 import json
 import math
 import os
@@ -37,19 +43,21 @@ from ttc_b200.replicas import job_throughput, max_over_ranks, rank_seed  # noqa:
 METRIC = "transpose GB/s (% of HBM peak); learned-vs-searched plan GB/s and tuning time"
 WORKLOAD = ("sweep64: 64 seeded rank-2..6 transpositions, |A|~200 MiB each, fp32/fp64, random "
             "non-identity perms, one extent in [7,31]; even cases alpha=1 beta=0, odd alpha=1.5 beta=-0.5")
+L2_NOTE = "inputs larger than L2 (|A| ~ 200 MiB per case); no flush needed"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cases", type=int, default=64)
-    ap.add_argument("--e2e-cases", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-sample-cases", type=int, default=6)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline: minimum seconds of timed passes")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations (README, strided, batched, selector) in the sweep line")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case", "configs"],
                     help="sweep: the 64-case 200 MiB sweep (default); batched: 4096 small transpositions "
@@ -65,7 +73,9 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-tuning", default="search", choices=["search", "default"],
                     help="per-problem schedules: measured search (the autotuner) or the planner default")
-    return ap.parse_args()
+    ap.add_argument("--selector-cases", type=int, default=12,
+                    help="held-out problems for the learned selector's fresh head to head")
+    return ap.parse_args(argv)
 
 
 # ------------------------------------------------------------------------------------------------
@@ -150,52 +160,93 @@ def ncu_traffic_per_gb(kernel: str):
     return float(m.group(1)) if m else None
 
 
+def kernel_name(desc: dict) -> str:
+    """The kernel that moves (almost) all of a plan's elements on its default path."""
+    if desc["kernel"] == "row":
+        return "row_kernel"
+    t = desc.get("tile") or {}
+    v = desc.get("tile_variant", 0)
+    if t.get("async") and v in (0, 3):
+        return "tile_async_kernel"
+    return "tile_fast_kernel" if (v == 2 or (v == 0 and t.get("fast"))) else "tile_kernel"
+
+
+def sweep_config(cases: int, bytes_per_step: int, world: int) -> dict:
+    """The `config` of the sweep line; both arms print the same one."""
+    return {"workload": WORKLOAD, "cases": cases, "bytes_per_step_per_gpu": bytes_per_step, "l2": L2_NOTE,
+            "parallelism": f"replicas x{world} (independent seeded sweeps, no collective)"}
+
+
 # ------------------------------------------------------------------------------------------------
-def cpu_prepare(cases):
-    """Seeded host inputs for the CPU baseline sample (untimed), 64-byte aligned."""
+# CPU baseline: the reference's own CPU implementation of the path on this host's cores
+def host_inputs(cases, threads):
+    """Seeded 32-byte aligned host inputs (A uniform[-1,1) from the case seed, B from seed + 1) for
+    the reference arm, filled in parallel."""
     from oracle.cpu_ref import aligned
-    out = []
-    for c in cases:
+
+    def one(c):
         real = np.float32 if c["dtype"] == "s" else np.float64
-        na = math.prod(c["size"])
-        A = aligned(na, real)
-        B = aligned(na, real)
-        A[:] = np.random.default_rng(c["seed"]).uniform(-1, 1, na)
-        B[:] = np.random.default_rng(c["seed"] + 1).uniform(-1, 1, na)
-        out.append((c, A, B))
-    return out
+        n = math.prod(c["size"])
+        A, B = aligned(n, real), aligned(n, real)
+        A[:] = np.random.default_rng(c["seed"]).uniform(-1, 1, n)
+        B[:] = np.random.default_rng(c["seed"] + 1).uniform(-1, 1, n)
+        return c, A, B
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        return list(ex.map(one, cases))
 
 
-def cpu_reference_run(prepared, threads, min_seconds=10.0, max_passes=50):
-    """Times the reference's CPU implementation on a bounded sample; returns (GB/s, kind, desc)."""
-    import oracle
-    from oracle import cpu_ref
+class CpuReference:
+    """TTC's generated AVX code for every case it was built for (rebuilt for this host with TTC's own
+    Makefile flags), and the C port of TTC's reference loop for any case it was not."""
+
+    def __init__(self, cases):
+        from oracle import cpu_ref
+        self.note = ""
+        try:
+            impl = cpu_ref.available(native=True)
+        except Exception as ex:  # a failed host build falls back to the portable build
+            impl = cpu_ref.available()
+            self.note = f"; host build failed ({type(ex).__name__}), portable build used"
+        self.impl = impl
+        self.covered = sum(1 for c in cases if impl is not None and cpu_ref._key(c) in impl.keys)
+        self.total = len(cases)
+        self.kind = "reference" if self.covered else "port"
+
+    def run(self, c, A, B, threads):
+        import oracle
+        from oracle import cpu_ref
+        if self.impl is not None and cpu_ref._key(c) in self.impl.keys:
+            self.impl(c, A, B, threads)
+        else:
+            oracle.transpose(A, B, c["perm"], c["size"], c["alpha"], c["beta"], dtype=c["dtype"], threads=threads)
+
+    def describe(self, threads) -> str:
+        if not self.covered:
+            return f"C port of TTC's OpenMP reference loop, {threads} threads" + self.note
+        i = self.impl
+        s = (f"TTC's generated AVX code, the variant TTC's own search picked per case (--maxImplementations="
+             f"{i.max_implementations}, searched on a {i.threads_at_tuning}-thread build host), compiled on this "
+             f"host with {i.flags} (compile {i.compile_seconds:.0f} s, outside the timing), {threads} threads")
+        if self.covered < self.total:
+            s += f"; {self.total - self.covered} of {self.total} cases by the C port of TTC's reference loop"
+        return s + self.note
+
+
+def cpu_passes(ref: CpuReference, prepared, threads, min_seconds=0.0, max_passes=1):
+    """Timed passes over every prepared case; returns (GB/s, passes, seconds)."""
     import ttc_b200.workloads as wl
-    impl = cpu_ref.available()
-    if impl is not None and not all(cpu_ref._key(c) in impl.keys for c, _, _ in prepared):
-        impl = None
-    kind = "reference" if impl else "port"
-    total_bytes, total_time = 0, 0.0
-    t_start = time.perf_counter()
-    passes = 0
-    while True:
-        for c, A, B in prepared:
-            t0 = time.perf_counter()
-            if impl:
-                impl(c, A, B, threads)
-            else:
-                oracle.transpose(A, B, c["perm"], c["size"], c["alpha"], c["beta"], dtype=c["dtype"],
-                                 threads=threads)
-            total_time += time.perf_counter() - t0
-            total_bytes += wl.case_bytes(c)
-        passes += 1
-        if time.perf_counter() - t_start >= min_seconds or passes >= max_passes:
-            break
     per_pass = sum(wl.case_bytes(c) for c, _, _ in prepared)
-    desc = (f"first {len(prepared)} sweep cases ({per_pass / 1e9:.2f} GB per pass) x {passes} passes, "
-            f"{threads} threads, " + ("TTC's generated AVX code (best variant of TTC's own search)"
-                                       if impl else "C port of TTC's OpenMP reference loop"))
-    return total_bytes / total_time / 1e9, kind, desc
+    total_t, passes = 0.0, 0
+    while True:
+        t0 = time.perf_counter()
+        for c, A, B in prepared:
+            ref.run(c, A, B, threads)
+        total_t += time.perf_counter() - t0
+        passes += 1
+        if total_t >= min_seconds or passes >= max_passes:
+            break
+    return per_pass * passes / total_t / 1e9, passes, total_t
 
 
 def run_reference_arm(args, rank, world):
@@ -203,45 +254,230 @@ def run_reference_arm(args, rank, world):
         return 0
     import ttc_b200.workloads as wl
     threads = os.cpu_count() or 1
-    cases = wl.sweep_cases(args.seed)[: max(1, args.cpu_sample_cases)]
-    prepared = cpu_prepare(cases)
+    cases = wl.sweep_cases(args.seed)[: args.cases]
+    ref = CpuReference(cases)
+    prepared = host_inputs(cases, threads)
     for _ in range(args.warmup):
-        cpu_reference_run(prepared[:1], threads, min_seconds=0.0, max_passes=1)
-    t0 = time.perf_counter()
-    vals = []
+        cpu_passes(ref, prepared, threads)
+    vals, t_all = [], 0.0
     for _ in range(args.steps):
-        v, kind, desc = cpu_reference_run(prepared, threads, min_seconds=0.0, max_passes=1)
+        v, _, t = cpu_passes(ref, prepared, threads)
         vals.append(v)
-    wall = time.perf_counter() - t0
+        t_all += t
     value = statistics.median(vals)
     total_bytes = sum(wl.case_bytes(c) for c in cases)
+    desc = ref.describe(threads) + f"; all {len(cases)} sweep cases per step, median of {args.steps} steps"
     line = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall / args.steps * 1e3, 3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_all / args.steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic (seeded uniform[-1,1])",
-            "config": {"workload": WORKLOAD, "sample_cases": len(cases), "bytes_per_step": total_bytes},
-            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                             "sample": desc + f"; median of {args.steps} steps"},
+            "data": "synthetic (seeded uniform[-1,1])", "config": sweep_config(len(cases), total_bytes, 1),
+            "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": ref.kind,
+                             "sample": desc},
             "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ------------------------------------------------------------------------------------------------
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference_arm(args, rank, world)
-    if args.workload == "batched":
-        return run_batched(args, rank, world, local)
-    if args.workload == "case":
-        return run_case(args)
-    if args.workload == "configs":
-        return run_configs(args)
+def parse_cpulist(text: str) -> set:
+    """CPU numbers of a Linux cpulist ("0-3,8,10-11")."""
+    cpus = set()
+    for part in text.strip().split(","):
+        if part:
+            lo, _, hi = part.partition("-")
+            cpus.update(range(int(lo), int(hi or lo) + 1))
+    return cpus
 
+
+class GpuLocalCpus:
+    """Runs its body on the CPUs of the GPU's own NUMA node (from the PCI device's `local_cpulist`),
+    so that pinned host buffers allocated there are first touched, and placed, on the memory next to
+    the GPU's PCIe root; the process's previous CPU set is restored afterwards. A no-op where the
+    node is not known."""
+
+    def __init__(self, dev):
+        self.dev, self.old = dev, None
+
+    def __enter__(self):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.dev)
+            path = Path(f"/sys/bus/pci/devices/{pr.pci_domain_id:04x}:{pr.pci_bus_id:02x}:"
+                        f"{pr.pci_device_id:02x}.0/local_cpulist")
+            cpus = parse_cpulist(path.read_text())
+            old = os.sched_getaffinity(0)
+            use = cpus & old
+            if use and use != old:
+                os.sched_setaffinity(0, use)
+                self.old = old
+        except (OSError, ValueError, AttributeError, RuntimeError):
+            self.old = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.old is not None:
+            os.sched_setaffinity(0, self.old)
+        return False
+
+
+def measure_pcie(dev, nbytes=1 << 30, reps=3):
+    """Pinned host<->device copy bandwidth of this GPU's link: each direction alone and both at once
+    (GB/s, best of `reps`, CUDA events)."""
+    import torch
+    with GpuLocalCpus(dev):
+        h_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        h_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            cur = torch.cuda.current_stream()
+            e0.record(cur)
+            s1.wait_stream(cur)
+            s2.wait_stream(cur)
+            fn()
+            cur.wait_stream(s1)
+            cur.wait_stream(s2)
+            e1.record(cur)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    def h2d():
+        with torch.cuda.stream(s1):
+            d_in.copy_(h_in, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(s2):
+            h_out.copy_(d_out, non_blocking=True)
+
+    def both():
+        h2d()
+        d2h()
+
+    h2d(), d2h()
+    t_in, t_out, t_both = timed(h2d), timed(d2h), timed(both)
+    gb = nbytes / 1e9
+    out = {"h2d_gbs": round(gb / (t_in / 1e3), 2), "d2h_gbs": round(gb / (t_out / 1e3), 2),
+           "duplex_gbs_each_way": round(gb / (t_both / 1e3), 2), "bytes": nbytes}
+    del h_in, h_out, d_in, d_out
+    return out
+
+
+def run_e2e(args, items, stream, dev, world, pcie):
+    """The metric through the public call from pinned host buffers, over every case of the sweep:
+    per case, A (and B when beta != 0) is copied in, transposed and B copied out. Copies in and out
+    run on their own streams so that PCIe carries both directions at once (case i+1 comes in while
+    case i goes out); each case's copy-in, kernel and copy-out are ordered by events. Results go to a
+    ring of four pinned output buffers. Returns (e2e dict, per-case host buffers)."""
+    import torch
+    host = []
+    with GpuLocalCpus(dev):  # pinned buffers on the host memory next to the GPU
+        for c, plan, A, B in items:
+            hA = torch.empty(A.numel(), dtype=A.dtype, pin_memory=True)
+            hA.copy_(A)
+            hB = None
+            if c["beta"] != 0:
+                hB = torch.empty(B.numel(), dtype=B.dtype, pin_memory=True)
+                hB.copy_(B)
+            host.append((hA, hB))
+        big = max(B.numel() * B.element_size() for _, _, _, B in items)
+        ring = [torch.empty(big, dtype=torch.uint8, pin_memory=True) for _ in range(4)]
+    h2d = sum(hA.numel() * hA.element_size() + (hB.numel() * hB.element_size() if hB is not None else 0)
+              for hA, hB in host)
+    d2h = sum(B.numel() * B.element_size() for _, _, _, B in items)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    out_done = [None] * len(items)  # per case: its last copy-out, before its device buffers are refilled
+    ring_done = [None] * len(ring)  # per ring slot: its last copy-out
+
+    def one():
+        for k, ((c, plan, A, B), (hA, hB)) in enumerate(zip(items, host)):
+            with torch.cuda.stream(s_in):
+                if out_done[k] is not None:
+                    s_in.wait_event(out_done[k])
+                A.copy_(hA, non_blocking=True)
+                if hB is not None:
+                    B.copy_(hB, non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(s_in)
+            stream.wait_event(ev_in)
+            plan(A, B, c["alpha"], c["beta"], stream)
+            ev_k = torch.cuda.Event()
+            ev_k.record(stream)
+            slot = k % len(ring)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_k)
+                nb = B.numel() * B.element_size()
+                ring[slot][:nb].copy_(B.view(torch.uint8), non_blocking=True)
+                out_done[k] = torch.cuda.Event()
+                out_done[k].record(s_out)
+                ring_done[slot] = out_done[k]
+        stream.wait_stream(s_out)
+
+    one()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    s_in.wait_stream(stream)
+    s_out.wait_stream(stream)
+    for _ in range(args.e2e_steps):
+        one()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(t0.elapsed_time(t1) / args.e2e_steps, dev)
+    nbytes = sum(p.bytes for _, p, _, _ in items)
+    out = {"value": round(nbytes * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "cases": len(items), "ms_per_step": round(ms, 3),
+           "note": ("pinned host A (and B when beta != 0) copied in and B copied out for every case inside the "
+                    "timed region; copy-in and copy-out on separate streams (PCIe both directions)")}
+    if pcie:
+        # the fastest the copies alone could go on this link: each direction at the rate it reaches while
+        # the other direction is busy (a lower bound on time, so an upper bound on e2e GB/s)
+        duplex = pcie["duplex_gbs_each_way"]
+        t_min = max(h2d, d2h) / (duplex * 1e9)
+        bound = nbytes / t_min / 1e9
+        out["pcie"] = pcie
+        out["pcie_bound_gbs"] = round(bound, 2)
+        out["frac_of_pcie_bound"] = round(out["value"] / world / bound, 4)
+    del ring
+    return out, host
+
+
+def cpu_baseline_on(items, host, threads, min_seconds):
+    """TTC's generated code over every sweep case, on the pinned host copies of the GPU inputs
+    (A; B where beta != 0, else a shared scratch buffer the code only writes)."""
+    cases = [c for c, _, _, _ in items]
+    ref = CpuReference(cases)
+    from oracle.cpu_ref import aligned
+    out_bytes = max([hA.numel() * hA.element_size() for hA, hB in host if hB is None] or [0])
+    scratch = aligned(max(out_bytes, 64), np.uint8)  # B of the beta == 0 cases: written, never read
+    prepared = []
+    for (c, _, _, _), (hA, hB) in zip(items, host):
+        a = hA.numpy()
+        b = hB.numpy() if hB is not None else scratch[: a.nbytes].view(a.dtype)
+        if a.ctypes.data % 32 or b.ctypes.data % 32:  # TTC's aligned vector accesses need 32 bytes
+            a2, b2 = aligned(a.size, a.dtype), aligned(b.size, b.dtype)
+            a2[:], b2[:] = a, b
+            a, b = a2, b2
+        prepared.append((c, a, b))
+    cpu_passes(ref, prepared, threads)  # warm-up pass
+    v, passes, secs = cpu_passes(ref, prepared, threads, min_seconds=min_seconds, max_passes=1000)
+    return {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": ref.kind,
+            "sample": (ref.describe(threads) + f"; all {len(prepared)} sweep cases per pass, {passes} passes in "
+                       f"{secs:.1f} s, on the same data as the GPU run")}
+
+
+# ------------------------------------------------------------------------------------------------
+def run_sweep(args, rank, world, local):
     import torch
     import torch.distributed as dist
     import ttc_b200.workloads as wl
@@ -258,6 +494,7 @@ def main():
     # resident inputs, seeded on the device
     gen = torch.Generator(device=dev)
     items = []
+    t_sel = 0.0
     for c in cases:
         n = math.prod(c["size"])
         gen.manual_seed(c["seed"])
@@ -268,14 +505,9 @@ def main():
         if args.schedule == "learned":
             from ttc_b200 import cost_model
             from ttc_b200.autotune import Problem
-            # the network's top-1; below its confidence threshold the top-1 and the planner default
-            # are timed (outside the timed region) and the faster one is kept
-            sel = cost_model.select(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]),
-                                    verify=False, measure_choice=False)
-            if sel["results"]:
-                tuning = min(sel["results"], key=lambda r: r.time_ms).tuning or None
-            else:
-                tuning = sel["candidates"][int(sel["order"][0])][0] or None
+            t0 = time.perf_counter()
+            tuning = cost_model.choose_tuning(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]))
+            t_sel += time.perf_counter() - t0
         plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=tuning)
         items.append((c, plan, A, B))
     torch.cuda.synchronize()
@@ -322,181 +554,110 @@ def main():
     value = job_throughput(bytes_per_step, world, ms_per_step)
 
     # per-kernel split of device time (dominant kernel -> roofline)
-    kinds = [p.describe()["kernel"] for _, p, _, _ in items]
+    descs = [p.describe() for _, p, _, _ in items]
+    kinds = [kernel_name(d) for d in descs]
     # a staged tile plan with ragged tiles also launches its edge plans (or the ragged-tile kernel)
     launches_per_step = sum(p.launches() for _, p, _, _ in items)
     per_kind = {}
-    for s in range(args.steps):
-        for k, (c, plan, A, B) in enumerate(items):
-            ms = evs[s][k][0].elapsed_time(evs[s][k][1])
-            d = per_kind.setdefault(kinds[k], [0.0, 0, 0])
-            d[0] += ms
-            d[1] += plan.bytes
-            d[2] += 1
+    per_case = []
+    for k, (c, plan, A, B) in enumerate(items):
+        ms = [evs[s][k][0].elapsed_time(evs[s][k][1]) for s in range(args.steps)]
+        d = per_kind.setdefault(kinds[k], [0.0, 0, 0])
+        d[0] += sum(ms)
+        d[1] += plan.bytes * args.steps
+        d[2] += args.steps
+        per_case.append(round(plan.bytes / (statistics.median(ms) / 1e3) / 1e9, 1))
     dom = max(per_kind, key=lambda k: per_kind[k][0])
     dom_ms, dom_bytes, dom_n = per_kind[dom]
     peak, peak_src = measured_peak_gbs()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    tr = ncu_traffic_per_gb(f"{dom}_kernel")
+    tr = ncu_traffic_per_gb(dom)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_src,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "kernel": f"{dom}_kernel",
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "kernel": dom,
                 "launches": dom_n, "algorithmic_bytes_per_launch": int(dom_bytes / dom_n),
                 "traffic": (int(tr * dom_bytes / dom_n) if tr else None),
                 "split": {k: {"ms": round(v[0], 3), "GBps": round(v[1] / (v[0] / 1e3) / 1e9, 1), "launches": v[2]}
-                          for k, v in per_kind.items()}}
+                          for k, v in per_kind.items()},
+                "per_case_GBps": per_case, "cases_below_0.7_of_peak": int(sum(g < 0.7 * peak for g in per_case))}
 
-    # end to end through the public call with pinned host buffers
-    e2e = run_e2e(args, items, stream, dev, world)
+    # end to end through the public call with pinned host buffers, over the same cases
+    pcie = measure_pcie(dev) if rank == 0 or world > 1 else None
+    e2e, host = run_e2e(args, items, stream, dev, world, pcie)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            prepared = cpu_prepare(cases[: max(1, args.cpu_sample_cases)])
-            v, kind, desc = cpu_reference_run(prepared, os.cpu_count() or 1, min_seconds=10.0)
-            cpu = {"value": round(v, 3), "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
+            cpu = cpu_baseline_on(items, host, os.cpu_count() or 1, args.cpu_seconds)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": "port",
                    "sample": f"failed: {ex}"}
+    del host
+    for _, p, _, _ in items:
+        p.close()
+    items.clear()
+    torch.cuda.empty_cache()
+
+    extras = {}
+    if world == 1 and not args.no_extras:
+        for name, fn in (("configs", lambda: configs_summary(args)), ("batched", lambda: batched_summary(args)),
+                         ("selector", lambda: selector_summary(args))):
+            try:
+                extras[name] = fn()
+            except Exception as ex:  # an extra never hides the headline
+                extras[name] = {"error": f"{type(ex).__name__}: {ex}"}
+            torch.cuda.empty_cache()
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded uniform[-1,1])",
                 "pct_of_hbm_peak": round(100 * value / world / peak, 2),
-                "config": {"workload": WORKLOAD, "cases": len(items), "bytes_per_step_per_gpu": bytes_per_step,
-                           "schedules": ("learned selector (top-1; timed against the planner default when its confidence "
-                                         "< 0.1)" if args.schedule == "learned" else "planner default"),
-                           "l2": "inputs larger than L2 (|A| ~ 200 MiB per case); no flush needed",
-                           "parallelism": f"replicas x{world} (independent seeded sweeps, no collective)"},
+                "config": sweep_config(len(cases), bytes_per_step, world),
+                "schedules": ("learned selector (top-1; timed against the planner default when its confidence "
+                              "< 0.1)" if args.schedule == "learned" else "planner default"),
+                "schedule_seconds": round(t_sel, 1),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "gpu_launches": launches_per_step * args.steps}
+                "gpu_launches": launches_per_step * args.steps, **extras}
         print(json.dumps(line), flush=True)
-    for _, p, _, _ in items:
-        p.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def parse_cpulist(text: str) -> set:
-    """CPU numbers of a Linux cpulist ("0-3,8,10-11")."""
-    cpus = set()
-    for part in text.strip().split(","):
-        if part:
-            lo, _, hi = part.partition("-")
-            cpus.update(range(int(lo), int(hi or lo) + 1))
-    return cpus
-
-
-class GpuLocalCpus:
-    """Runs its body on the CPUs of the GPU's own NUMA node (from the PCI device's `local_cpulist`),
-    so that pinned host buffers allocated there are first touched, and placed, on the memory next to
-    the GPU's PCIe root; the process's previous CPU set is restored afterwards. A no-op where the
-    node is not known."""
-
-    def __init__(self, dev):
-        self.dev, self.old = dev, None
-
-    def __enter__(self):
-        import torch
-        try:
-            pr = torch.cuda.get_device_properties(self.dev)
-            path = Path(f"/sys/bus/pci/devices/{pr.pci_domain_id:04x}:{pr.pci_bus_id:02x}:"
-                        f"{pr.pci_device_id:02x}.0/local_cpulist")
-            cpus = parse_cpulist(path.read_text())
-            old = os.sched_getaffinity(0)
-            use = cpus & old
-            if use and use != old:
-                os.sched_setaffinity(0, use)
-                self.old = old
-        except (OSError, ValueError, AttributeError, RuntimeError):
-            self.old = None
-        return self
-
-    def __exit__(self, *exc):
-        if self.old is not None:
-            os.sched_setaffinity(0, self.old)
-        return False
-
-
-def run_e2e(args, items, stream, dev, world):
-    """The metric through the public call from pinned host buffers: per case, A (and B when
-    beta != 0) is copied in, transposed and B copied out. Copies in and out run on their own
-    streams so that PCIe carries both directions at once (case i+1 comes in while case i goes out);
-    each case's copy-in, kernel and copy-out are ordered by events."""
+# ------------------------------------------------------------------------------------------------
+def flushed_timing(plan, A, B, alpha, beta, steps, warmup, flush):
+    """Median and best ms of `steps` launches, each after writing 2x the L2 (CUDA events)."""
     import torch
-    sub = items[: max(1, min(args.e2e_cases, len(items)))]
-    host = []
-    with GpuLocalCpus(dev):  # pinned buffers on the host memory next to the GPU
-        for c, plan, A, B in sub:
-            hA = torch.empty(A.numel(), dtype=A.dtype, pin_memory=True)
-            hB = torch.empty(B.numel(), dtype=B.dtype, pin_memory=True)
-            hA.copy_(A)
-            hB.copy_(B)
-            host.append((hA, hB))
-        outs = [torch.empty_like(hB, pin_memory=True) for _, hB in host]
-    h2d = sum(hA.numel() * hA.element_size() + (hB.numel() * hB.element_size() if c["beta"] != 0 else 0)
-              for (c, _, _, _), (hA, hB) in zip(sub, host))
-    d2h = sum(hB.numel() * hB.element_size() for _, hB in host)
-    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    out_done = [None] * len(sub)  # per case: its last copy-out, before its buffers are refilled
-
-    def one():
-        for k, ((c, plan, A, B), (hA, hB), o) in enumerate(zip(sub, host, outs)):
-            with torch.cuda.stream(s_in):
-                if out_done[k] is not None:
-                    s_in.wait_event(out_done[k])
-                A.copy_(hA, non_blocking=True)
-                if c["beta"] != 0:
-                    B.copy_(hB, non_blocking=True)
-                ev_in = torch.cuda.Event()
-                ev_in.record(s_in)
-            stream.wait_event(ev_in)
-            plan(A, B, c["alpha"], c["beta"], stream)
-            ev_k = torch.cuda.Event()
-            ev_k.record(stream)
-            with torch.cuda.stream(s_out):
-                s_out.wait_event(ev_k)
-                o.copy_(B, non_blocking=True)
-                out_done[k] = torch.cuda.Event()
-                out_done[k].record(s_out)
-        stream.wait_stream(s_out)
-
-    one()
-    torch.cuda.synchronize()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    s_in.wait_stream(stream)
-    s_out.wait_stream(stream)
-    for _ in range(args.e2e_steps):
-        one()
-    t1.record(stream)
-    torch.cuda.synchronize()
-    ms = max_over_ranks(t0.elapsed_time(t1) / args.e2e_steps, dev)
-    nbytes = sum(p.bytes for _, p, _, _ in sub)
-    return {"value": round(nbytes * world / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "cases": len(sub), "ms_per_step": round(ms, 3),
-            "note": ("pinned host A (and B when beta != 0) copied in and B copied out for every case inside the "
-                     "timed region; copy-in and copy-out on separate streams (PCIe both directions)")}
+    for _ in range(warmup):
+        plan(A, B, alpha, beta)
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan(A, B, alpha, beta)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.median(ms), min(ms)
 
 
-def run_configs(args):
+def configs_summary(args, steps=None, warmup=None):
     """The single-problem configurations: TTC's README shape (perm 1,0,2 / 1000,768,16, fp32,
     alpha = beta = 1) and the strided mixed-precision shape (perm 3,1,0,2 / 96,80,72,64, lda + 8,0,4,0;
     z->c with alpha = (0.5, 0.25) and d->s with alpha = 0.5, beta = 0). Inputs uniform[-1,1] from the
     seed (B from seed + 1), resident; the L2 is flushed (2x its size written) before every timed
-    launch; CUDA events, `--steps` launches after `--warmup`. Prints one JSON line."""
+    launch; CUDA events. Returns {name: result}."""
     import torch
     import ttc_b200.workloads as wl
     from ttc_b200 import Plan
+    steps = steps or max(args.steps, 10)
+    warmup = warmup or max(args.warmup, 3)
     tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
     flush = torch.empty(2 * 126 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    out = []
+    peak, _ = measured_peak_gbs()
+    out = {}
     for name, c in [("readme_1000x768x16_s_beta1", wl.readme_case())] + \
                    [(f"strided_96x80x72x64_{c['dtype']}", c) for c in wl.strided_cases()]:
         ta, tb = (c["dtype"][0], c["dtype"][1]) if len(c["dtype"]) == 2 else (c["dtype"], c["dtype"])
@@ -509,32 +670,105 @@ def run_configs(args):
         gen.manual_seed(args.seed + 1)
         B = (torch.rand(nb, dtype=tmap[tb], device="cuda", generator=gen) * 2 - 1)
         plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, lda=c.get("lda"))
-        for _ in range(args.warmup):
-            plan(A, B, c["alpha"], c["beta"])
-        ms = []
-        for _ in range(args.steps):
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            plan(A, B, c["alpha"], c["beta"])
-            e1.record()
-            torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        med = statistics.median(ms)
-        peak, src = measured_peak_gbs()
+        med, best = flushed_timing(plan, A, B, c["alpha"], c["beta"], steps, warmup, flush)
         d = plan.describe()
-        out.append({"config": name, "perm": c["perm"], "size": c["size"], "lda": c.get("lda"), "dtype": c["dtype"],
-                    "alpha": str(c["alpha"]), "beta": c["beta"], "bytes": plan.bytes,
-                    "GBps_median": round(plan.bytes / (med / 1e3) / 1e9, 1),
-                    "GBps_best": round(plan.bytes / (min(ms) / 1e3) / 1e9, 1),
-                    "pct_of_hbm_peak": round(100 * plan.bytes / (med / 1e3) / 1e9 / peak, 1),
-                    "kernel": d["kernel"], "tile": d.get("tile"), "vec": [d["vecA"], d["vecB"]]})
+        gbs = plan.bytes / (med / 1e3) / 1e9
+        out[name] = {"perm": c["perm"], "size": c["size"], "lda": c.get("lda"), "dtype": c["dtype"],
+                     "alpha": str(c["alpha"]), "beta": c["beta"], "bytes": plan.bytes,
+                     "GBps_median": round(gbs, 1), "GBps_best": round(plan.bytes / (best / 1e3) / 1e9, 1),
+                     "frac_of_hbm_peak": round(gbs / peak, 4), "kernel": kernel_name(d), "tile": d.get("tile"),
+                     "vec": [d["vecA"], d["vecB"]], "l2": "flushed before every launch", "steps": steps}
         plan.close()
-    print(json.dumps({"workload": "configs", "steps": args.steps, "warmup": args.warmup, "l2": "flushed",
-                      "results": out}), flush=True)
-    return 0
+    return out
 
 
+def batched_summary(args):
+    """The batched workload (4096 problems) in one persistent launch replayed from a CUDA graph,
+    against the same problems as a CUDA graph of per-call launches; every batched result compared bit
+    for bit with the per-call result. Returns a dict."""
+    import torch
+    from ttc_b200.batched import Batch
+    plans, As, Bs, Cs, t_tune, cases = build_batch_problems(args, 0, torch.device("cuda"))
+    batch = Batch(plans, As, Bs, alpha=1.0)
+    stream = torch.cuda.current_stream()
+    total = batch.bytes
+    g = capture_per_call(plans, As, Cs, stream)
+    for _ in range(3):
+        batch.launch(stream, graph=True)
+        g.replay()
+    batch.check_status(stream)
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_b = timed(lambda: batch.launch(stream, graph=True), 10)
+    ms_c = timed(g.replay, 10)
+    batch.check_status(stream)
+    torch.cuda.synchronize()
+    mismatches = sum(0 if torch.equal(b.view(torch.int32), cbuf.view(torch.int32)) else 1 for b, cbuf in zip(Bs, Cs))
+    gbs = lambda ms: round(total / (ms / 1e3) / 1e9, 1)
+    del g
+    batch.close()
+    for p in plans:
+        p.close()
+    return {"workload": BATCH_WORKLOAD, "problems": len(cases), "bytes": total,
+            "batched_graph_GBps": gbs(ms_b), "graph_of_per_call_launches_GBps": gbs(ms_c),
+            "speedup_vs_graph_of_calls": round(ms_c / ms_b, 2), "tuning_seconds": round(t_tune, 1),
+            "mismatches_vs_per_call": mismatches, "steps": 10}
+
+
+def selector_summary(args):
+    """The learned selector against a fresh measured search on held-out problems (the first
+    `--selector-cases` problems of the held-out seed, 1-256 MiB): per problem, every candidate is
+    timed (the exhaustive search), then the search's winner, the network's top-1 and the planner
+    default are re-timed alternately (so the winner loses the bias of being the maximum of noisy
+    timings); tuning time is the search's wall time against the selector's (planning, features,
+    inference, and its timed fallback when unsure)."""
+    import ttc_b200.workloads as wl
+    from ttc_b200 import cost_model
+    from ttc_b200.autotune import Bench, Problem, measure, search
+    model = cost_model.load_default()
+    rows = []
+    for c in wl.learning_cases(cost_model.HELDOUT_SEED, args.selector_cases):
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        sr = search(p, max_impl=64, reps=3, verify=False)
+        sel_top1 = cost_model.select(p, confidence=0.0, model=model, verify=False, measure_choice=False)
+        sel = cost_model.select(p, model=model, verify=False, measure_choice=False)
+        top1 = sel_top1["candidates"][int(sel_top1["order"][0])][0]
+        chosen = min(sel["results"], key=lambda r: r.time_ms).tuning if sel["results"] else top1
+        picks = [sr["best"].tuning, top1, chosen, {}]
+        bench = Bench(p, seed=1)
+        best_ms = [float("inf")] * len(picks)
+        for rnd in range(2):
+            order = list(range(len(picks))) if rnd == 0 else list(reversed(range(len(picks))))
+            for i, r in zip(order, measure(p, [picks[i] for i in order], reps=5, verify=False, bench=bench)):
+                best_ms[i] = min(best_ms[i], r.time_ms)
+        del bench
+        rows.append({"search_s": sr["seconds"], "top1_s": sel_top1["seconds"], "sel_s": sel["seconds"],
+                     "top1": best_ms[0] / best_ms[1], "sel": best_ms[0] / best_ms[2], "dflt": best_ms[0] / best_ms[3],
+                     "fallback": bool(sel["fallback"])})
+    m = lambda k: float(np.mean([r[k] for r in rows]))
+    return {"problems": len(rows), "held_out_seed": cost_model.HELDOUT_SEED, "search_candidates": 64,
+            "top1_over_search": round(m("top1"), 4), "selector_over_search": round(m("sel"), 4),
+            "default_over_search": round(m("dflt"), 4),
+            "selector_within_5pct": round(float(np.mean([r["sel"] >= 0.95 for r in rows])), 4),
+            "fallbacks": int(sum(r["fallback"] for r in rows)),
+            "search_seconds_mean": round(m("search_s"), 3), "selector_seconds_mean": round(m("sel_s"), 4),
+            "top1_seconds_mean": round(m("top1_s"), 4),
+            "tuning_time_ratio_selector": round(m("search_s") / max(m("sel_s"), 1e-9), 1),
+            "tuning_time_ratio_top1": round(m("search_s") / max(m("top1_s"), 1e-9), 1),
+            "timing": "fresh: winner, top-1, selector choice and default re-timed alternately, best of 2x5 launches"}
+
+
+# ------------------------------------------------------------------------------------------------
 def run_case(args):
     """One sweep case, `--reps` launches of its default plan on seeded resident inputs; prints the
     plan and the mean GB/s (CUDA events). Meant to sit under a profiler."""
@@ -563,29 +797,25 @@ def run_case(args):
     return 0
 
 
+def run_configs(args):
+    out = configs_summary(args)
+    print(json.dumps({"workload": "configs", "steps": max(args.steps, 10), "warmup": max(args.warmup, 3),
+                      "l2": "flushed", "results": list(out.values())}), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------------------------------------
 BATCH_WORKLOAD = ("batched4096: seeded rank-3..5 fp32 transpositions, random perms, element counts "
                   "log-normal median 64Ki clipped to [1Ki, 1Mi], alpha=1 beta=0")
 
 
-def run_batched(args, rank, world, local):
-    """Batched mode: every problem of the batch in one persistent launch (plain and replayed from a
-    captured CUDA graph) against the same problems launched one call at a time: a Python loop over
-    the public call, that loop captured into a CUDA graph, and a loop that synchronizes after every
-    call as TTC's generated wrapper does. Every batched result is compared bit for bit with the
-    per-call result."""
+def build_batch_problems(args, rank, dev):
+    """Plans (with per-problem schedules from the measured search), seeded A, and NaN-filled B and C
+    buffers of the batched workload. Returns (plans, As, Bs, Cs, tuning seconds, cases)."""
     import torch
-    import torch.distributed as dist
     import ttc_b200.workloads as wl
     from ttc_b200 import Plan
-    from ttc_b200.autotune import Bench, Problem, tune_for_batch
-    from ttc_b200.batched import Batch
-
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
+    from ttc_b200.autotune import Problem, tune_for_batch
     cases = wl.batched_cases(seed=rank_seed(7, rank), count=args.batch_count)
     t_tune = time.perf_counter()
     plans, As, Bs, Cs = [], [], [], []
@@ -600,7 +830,41 @@ def run_batched(args, rank, world, local):
         As.append(torch.rand(n, device=dev, generator=gen).mul_(2).sub_(1))
         Bs.append(torch.full((n,), float("nan"), device=dev))
         Cs.append(torch.full((n,), float("nan"), device=dev))
-    t_tune = time.perf_counter() - t_tune
+    return plans, As, Bs, Cs, time.perf_counter() - t_tune, cases
+
+
+def capture_per_call(plans, As, Cs, stream):
+    """A CUDA graph of every problem's own per-call launch (into Cs)."""
+    import torch
+    g = torch.cuda.CUDAGraph()
+    s2 = torch.cuda.Stream()
+    s2.wait_stream(stream)
+    with torch.cuda.stream(s2):
+        for p, a, cbuf in zip(plans, As, Cs):  # warm the plans' launch paths before capture
+            p(a, cbuf, 1.0, 0.0, s2)
+        with torch.cuda.graph(g, stream=s2):
+            for p, a, cbuf in zip(plans, As, Cs):
+                p(a, cbuf, 1.0, 0.0, s2)
+    stream.wait_stream(s2)
+    return g
+
+
+def run_batched(args, rank, world, local):
+    """Batched mode: every problem of the batch in one persistent launch (plain and replayed from a
+    captured CUDA graph) against the same problems launched one call at a time: a Python loop over
+    the public call, that loop captured into a CUDA graph, and a loop that synchronizes after every
+    call as TTC's generated wrapper does. Every batched result is compared bit for bit with the
+    per-call result."""
+    import torch
+    import torch.distributed as dist
+    from ttc_b200.batched import Batch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    plans, As, Bs, Cs, t_tune, cases = build_batch_problems(args, rank, dev)
     batch = Batch(plans, As, Bs, alpha=1.0)
     total = batch.bytes
     stream = torch.cuda.current_stream()
@@ -632,14 +896,7 @@ def run_batched(args, rank, world, local):
         batch.launch(stream, graph=True)
         per_call()
     batch.check_status(stream)
-    g = torch.cuda.CUDAGraph()
-    s2 = torch.cuda.Stream()
-    s2.wait_stream(stream)
-    with torch.cuda.stream(s2):
-        with torch.cuda.graph(g, stream=s2):
-            for p, a, cbuf in zip(plans, As, Cs):
-                p(a, cbuf, 1.0, 0.0, s2)
-    stream.wait_stream(s2)
+    g = capture_per_call(plans, As, Cs, stream)
     for _ in range(args.warmup):
         g.replay()
     torch.cuda.synchronize()
@@ -692,6 +949,23 @@ def run_batched(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return 1 if mismatches else 0
+
+
+# ------------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if args.workload == "batched":
+        return run_batched(args, rank, world, local)
+    if args.workload == "case":
+        return run_case(args)
+    if args.workload == "configs":
+        return run_configs(args)
+    return run_sweep(args, rank, world, local)
 
 
 if __name__ == "__main__":

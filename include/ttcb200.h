@@ -103,9 +103,12 @@ ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const 
  * TTC, whose every call allocates. Plans on the host and writes the plan's descriptor into a 64 KiB
  * scratch array built into the library (held by every GPU that loads the library until exit);
  * never calls cudaMalloc/cudaFree. Uses the staged tile kernel; beta == NULL means beta = 0.
- * Problems whose descriptor exceeds the scratch size fail with TTCB_ERR_UNSUPPORTED. Calls that
- * overlap on the GPU race on the scratch array; calls in order on one stream do not. The first call
- * on each device looks up the scratch address and should come before any stream capture. */
+ * Problems whose descriptor exceeds the scratch size fail with TTCB_ERR_UNSUPPORTED (with the
+ * planner's tile limits a descriptor stays under about 34 KiB). Calls that overlap on the GPU race
+ * on the scratch array; calls in order on one stream do not. The first call on each device looks up
+ * the scratch address and should come before any stream capture. The descriptor is uploaded from
+ * host memory that lives only during the call, so a call on a stream that is being captured is
+ * refused with TTCB_ERR_UNSUPPORTED before anything is enqueued. */
 ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const int64_t* size, const int64_t* lda,
                                    const int64_t* ldb, ttcb_dtype type_a, ttcb_dtype type_b,
                                    const void* A, void* B, const void* alpha, const void* beta,

@@ -126,4 +126,5 @@ def main(ttc_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    from oracle.make_ref import DEFAULT_SOURCE
+    main(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SOURCE)

@@ -76,3 +76,46 @@ def test_batch_rejects_mixed_types():
     y = torch.zeros(64, device="cuda", dtype=torch.float32)
     with pytest.raises(TTCError):
         Batch([Plan([1, 0], [8, 8], "s"), Plan([1, 0], [8, 8], "d")], [y, x], [y, x])
+
+
+def test_full_batched_workload_matches_oracle():
+    """The batched workload the benchmark times, at full size: 4096 rank-3..5 fp32 problems with
+    log-normal element counts (median 64 Ki, 1 Ki..1 Mi), each with the schedule the autotuner's
+    measured search picks for it, in one persistent launch replayed from a CUDA graph. Every problem
+    is compared bit for bit with the oracle (TTC's reference loop, GPUreference.py:90-137 in the
+    TTC project) and with the per-call result of its own plan."""
+    import math
+    import os
+    import torch
+    import ttc_b200.workloads as wl
+    from ttc_b200 import Plan
+    from ttc_b200.autotune import Problem, tune_for_batch
+    from ttc_b200.batched import Batch
+    cases = wl.batched_cases(seed=7, count=4096)
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    plans, As, Bs, Cs = [], [], [], []
+    for k, c in enumerate(cases):
+        n = math.prod(c["size"])
+        tu = tune_for_batch(Problem(c["perm"], c["size"], "s"), max_impl=6, reps=2) or None
+        plans.append(Plan(c["perm"], c["size"], "s", False, tuning=tu))
+        gen.manual_seed(1_000_000 + k)
+        As.append(torch.rand(n, device=dev, generator=gen).mul_(2).sub_(1))
+        Bs.append(torch.full((n,), float("nan"), device=dev))
+        Cs.append(torch.full((n,), float("nan"), device=dev))
+    batch = Batch(plans, As, Bs, alpha=1.0)
+    batch.launch(graph=True)
+    batch.launch(graph=True)  # a replay on reset counters
+    batch.check_status()
+    for p, a, cbuf in zip(plans, As, Cs):
+        p(a, cbuf, 1.0, 0.0)
+    torch.cuda.synchronize()
+    threads = os.cpu_count() or 1
+    for k, c in enumerate(cases):
+        a = As[k].cpu().numpy()
+        want = oracle.transpose(a, np.zeros_like(a), c["perm"], c["size"], 1.0, 0.0, dtype="s", threads=threads)
+        assert_bitexact(Bs[k].cpu().numpy(), want, f"batched problem {k} {c} plan={plans[k].describe()}")
+        assert torch.equal(Bs[k].view(torch.int32), Cs[k].view(torch.int32)), f"problem {k}: batch vs per-call"
+    batch.close()
+    for p in plans:
+        p.close()

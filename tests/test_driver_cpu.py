@@ -52,8 +52,15 @@ def test_fuse_indices_mirror_matches_reference_restatement():
         perm = [int(x) for x in rng.permutation(r)]
         s1, p1, l1, b1 = list(size), list(perm), [], []
         ttc_util.fuseIndices(s1, p1, [], l1, b1)
+        # empty (dense) lda/ldb stay empty in the caller's lists, as in TTC (ttc_util.py:214-222)
+        assert (l1, b1) == ([], [])
+        l1, b1 = ttc_util.denseLeadingDims(s1, p1, l1, b1)
         s2, p2, l2, b2 = ref.fuse_indices(size, perm)
         assert (s1, p1, l1, b1) == (s2, p2, l2, b2)
+        # explicit leading dimensions are fused in place
+        s3, p3, l3, b3 = list(size), list(perm), list(size), [size[p] for p in perm]
+        ttc_util.fuseIndices(s3, p3, [], l3, b3)
+        assert (s3, p3, l3, b3) == (s2, p2, l2, b2)
 
 
 def test_cost_loop_mirror():

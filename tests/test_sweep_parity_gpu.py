@@ -1,0 +1,72 @@
+"""Parity of the headline workload at the size it is timed at.
+
+Every case of the 64-case sweep that the benchmark times (seed 2024: rank 2..6, fp32/fp64, |A| ~
+200 MiB, one extent in [7, 31]; even cases alpha = 1 beta = 0, odd cases alpha = 1.5 beta = -0.5) runs
+through the public Plan call with the planner's default schedule and with the learned selector's
+schedule (the one the benchmark uses), on the benchmark's own seeded device inputs, and is compared
+bit for bit with the oracle: the restated reference loop of TTC's CUDA path (GPUreference.py:90-137
+in the TTC project), in its OpenMP form. A canary after B catches writes past its end. Cases run one
+at a time, so the device holds one case's A, B and result at once.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(c, dev):
+    """The benchmark's inputs: uniform[-1, 1) from torch's CUDA generator seeded with the case seed
+    (A) and seed + 1 (B)."""
+    import torch
+    tmap = {"s": torch.float32, "d": torch.float64}
+    n = math.prod(c["size"])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(c["seed"])
+    A = torch.rand(n, dtype=tmap[c["dtype"]], device=dev, generator=gen).mul_(2).sub_(1)
+    gen.manual_seed(c["seed"] + 1)
+    B = torch.empty(n + 64, dtype=tmap[c["dtype"]], device=dev)
+    B[:n] = torch.rand(n, dtype=tmap[c["dtype"]], device=dev, generator=gen).mul_(2).sub_(1)
+    B[n:] = 7.0  # canary
+    return A, B
+
+
+@pytest.mark.parametrize("schedule", ["default", "learned"])
+def test_sweep64_full_size_matches_oracle(schedule):
+    import torch
+    import ttc_b200.workloads as wl
+    from ttc_b200 import Plan
+    from ttc_b200.autotune import Problem
+    from helpers import assert_bitexact
+    dev = torch.device("cuda", 0)
+    threads = os.cpu_count() or 1
+    checked = 0
+    for k, c in enumerate(wl.sweep_cases(2024)):
+        tuning = None
+        if schedule == "learned":
+            from ttc_b200 import cost_model
+            tuning = cost_model.choose_tuning(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]))
+            if tuning is None:
+                continue  # the planner default, checked by the other schedule
+        A, B = _inputs(c, dev)
+        n = A.numel()
+        hA = A.cpu().numpy()
+        want = B[:n].cpu().numpy().copy()
+        oracle.transpose(hA, want, c["perm"], c["size"], c["alpha"], c["beta"], dtype=c["dtype"], threads=threads)
+        plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=tuning)
+        plan(A, B[:n], c["alpha"], c["beta"])
+        torch.cuda.synchronize()
+        got = B.cpu().numpy()
+        assert np.all(got[n:] == 7.0), f"case {k}: write past the end of B"
+        assert_bitexact(got[:n], want, f"sweep case {k} {c} schedule={schedule} tuning={tuning} "
+                                       f"plan={plan.describe()}")
+        plan.close()
+        checked += 1
+        del A, B
+    torch.cuda.empty_cache()
+    if schedule == "default":
+        assert checked == 64

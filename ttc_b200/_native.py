@@ -86,6 +86,7 @@ TEST_SYMBOLS = [
     ("ttcb_test_plan_shapes", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_int, ctypes.c_char_p,
                                                 ctypes.c_size_t]),
+    ("ttcb_test_noalloc_limit", ctypes.c_size_t, [ctypes.c_size_t]),
     ("ttcb_test_plan_edges", ctypes.c_size_t, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_char_p, ctypes.c_size_t]),
 ]

@@ -427,6 +427,23 @@ def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, v
             "candidates": cands, "seconds_model": t_model, "seconds": time.perf_counter() - t0}
 
 
+# seeds of the training problems and of the held-out problems (ttc_b200.workloads.learning_cases)
+TRAIN_SEED = 11
+HELDOUT_SEED = 12345
+
+
+def choose_tuning(p: Problem, model: Optional[MLP] = None) -> Optional[dict]:
+    """The learned selector's schedule for one problem, as the benchmark uses it: the network's
+    top-1, or - below its confidence threshold - the faster of that and the planner default (timed
+    on the GPU with the problem's own inputs). None means the planner default."""
+    sel = select(p, verify=False, measure_choice=False, model=model)
+    if sel["results"]:
+        tu = min(sel["results"], key=lambda r: r.time_ms).tuning
+    else:
+        tu = sel["candidates"][int(sel["order"][0])][0]
+    return tu or None
+
+
 # ------------------------------------------------------------------------------------------------
 def collect(cases: list[dict], out: Path, max_impl: int = 64, reps: int = 3, log=print,
             deadline: Optional[float] = None) -> bool:
@@ -601,8 +618,8 @@ def main(argv=None):
     test_path = Path(a.corpus + "_test.npz")
     if a.cmd == "collect":
         deadline = time.time() + a.max_seconds if a.max_seconds else None
-        if collect(wl.learning_cases(11, a.train_cases), train_path, a.max_impl, deadline=deadline):
-            collect(wl.learning_cases(12345, a.test_cases), test_path, a.max_impl, deadline=deadline)
+        if collect(wl.learning_cases(TRAIN_SEED, a.train_cases), train_path, a.max_impl, deadline=deadline):
+            collect(wl.learning_cases(HELDOUT_SEED, a.test_cases), test_path, a.max_impl, deadline=deadline)
     elif a.cmd == "train":
         z = np.load(train_path)
         X, case = corpus_features(json.loads(bytes(z["meta"]).decode()))

@@ -54,11 +54,13 @@ static ttcb_status cuda_fail(cudaError_t e, const char* what) {
 
 static int variant_of(const ttcb_plan* p) { return p->beta_nonzero ? 2 : (p->streaming ? 1 : 0); }
 
+namespace ttcb {
 // Kernels whose shared memory (dynamic, plus the staged kernel's static descriptor header and tile
-// ring) may exceed the 48 KB default get the opt-in once per device.
-static bool needs_large_smem(int dynamic_smem) { return dynamic_smem + (int)ttcb::kAsyncStaticSmem > 48 * 1024; }
+// ring) may exceed the 48 KB default get the opt-in once per device, always to the planner's
+// ceiling (kMaxDynamicSmem), so that no caller ever lowers the limit another plan relies on.
+bool needs_large_smem(int dynamic_smem) { return dynamic_smem + (int)kAsyncStaticSmem > 48 * 1024; }
 
-static void allow_large_smem(const void* func) {
+void allow_large_smem(const void* func) {
   static std::mutex mu;
   static std::vector<std::pair<const void*, int>> done;
   int dev = 0;
@@ -66,10 +68,14 @@ static void allow_large_smem(const void* func) {
   std::lock_guard<std::mutex> lk(mu);
   for (const auto& x : done)
     if (x.first == func && x.second == dev) return;
-  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   cudaGetLastError();
   done.emplace_back(func, dev);
 }
+}  // namespace ttcb
+
+using ttcb::allow_large_smem;
+using ttcb::needs_large_smem;
 
 static ttcb_status plan_finish_device(ttcb_plan* p) {
   if (p->empty) return TTCB_OK;

@@ -225,7 +225,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
     return bfail(TTCB_ERR_DTYPE, "no batched kernel for this type pair");
   }
   if (b->smem + (int)sizeof(TileDesc) + 64 > 48 * 1024)  // + its static header copy, item and problem index
-    cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    ttcb::allow_large_smem(k.func);
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.func, ttcb::kThreads, b->smem);

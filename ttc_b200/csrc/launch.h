@@ -19,6 +19,14 @@ struct KernelRef {
 // One definition per A/B type pair lives in kernels_<pair>.cu.
 KernelRef pick_kernel(ttcb_dtype ta, ttcb_dtype tb, int kernel, int va, int vb, int variant);
 
+// Dynamic shared memory ceiling of every plan (the planner never exceeds it).
+constexpr int kMaxDynamicSmem = 200 * 1024;
+// True when a launch with this much dynamic shared memory needs the opt-in above 48 KB.
+bool needs_large_smem(int dynamic_smem);
+// Raises func's dynamic shared memory limit to kMaxDynamicSmem on the current device, once; it
+// never lowers it. Every entry point that launches a kernel goes through this (defined in abi.cu).
+void allow_large_smem(const void* func);
+
 using BatchLaunchFn = cudaError_t (*)(const void* probs, const int64_t* prefix, int count, unsigned long long total,
                                       unsigned long long* counter, int* status, const void* alpha, const void* beta,
                                       int blocks, int smem, int slots_bytes, int chunk, cudaStream_t stream);

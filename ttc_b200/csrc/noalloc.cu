@@ -15,6 +15,15 @@
 // On the first call on each device this entry point looks up the device address of the array with
 // cudaGetSymbolAddress (the symbol's name is only a host-side stand-in, not a device address). That
 // first call on a device should therefore come before any stream capture.
+//
+// The descriptor reaches the scratch array through a cudaMemcpyAsync from host memory that exists
+// only while the call runs. A call made while its stream is being captured would record a copy node
+// that reads that host memory again at every replay, long after it was freed, so such a call is
+// refused with TTCB_ERR_UNSUPPORTED before anything is enqueued.
+//
+// The kernels' dynamic shared memory limit is raised through the same once-per-device opt-in as
+// the plan entry points use (ttcb::allow_large_smem), which never lowers a limit that a plan made
+// earlier relies on.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -28,6 +37,10 @@
 
 static constexpr size_t kNoAllocScratchBytes = 64 * 1024;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Largest descriptor the entry point accepts: the scratch size, or less when a CPU test lowers it
+// (ttcb_test_noalloc_limit) to reach the rejection path with an ordinary problem.
+static size_t g_noalloc_limit = kNoAllocScratchBytes;
 
 extern "C" void ttcb_internal_set_error(const char* msg);
 
@@ -83,21 +96,28 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   if (p.empty) return TTCB_OK;
   const TileDesc* td = reinterpret_cast<const TileDesc*>(p.host_desc.data());
   if (!td->async_ok) return na_fail(TTCB_ERR_UNSUPPORTED, "problem needs offsets beyond 32 bits");
-  if (p.host_desc.size() > kNoAllocScratchBytes)
+  if (p.host_desc.size() > g_noalloc_limit)
     return na_fail(TTCB_ERR_UNSUPPORTED, "descriptor needs " + std::to_string(p.host_desc.size()) +
                                              " bytes of scratch; the no-allocation entry point holds at most " +
-                                             std::to_string(kNoAllocScratchBytes));
+                                             std::to_string(g_noalloc_limit));
   const int EA = dtype_bytes(p.ta), EB = dtype_bytes(p.tb);
   const int natA = (p.ta == TTCB_C) ? 8 : EA, natB = (p.tb == TTCB_C) ? 8 : EB;
   if ((uintptr_t)A % natA || (uintptr_t)B % natB)
     return na_fail(TTCB_ERR_ALIGN, "A or B is not aligned to its element size");
 
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return na_cuda(e, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return na_fail(TTCB_ERR_UNSUPPORTED,
+                   "ttcb_transpose_noalloc cannot be called while its stream is being captured: it uploads the "
+                   "descriptor from host memory that exists only during the call");
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return na_cuda(e, "cudaGetDevice");
   void* scratch = nullptr;
   if ((s = scratch_address(dev, &scratch)) != TTCB_OK) return s;
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   e = cudaMemcpyAsync(scratch, p.host_desc.data(), p.host_desc.size(), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return na_cuda(e, "descriptor upload to the scratch array");
   p.dev_desc = scratch;
@@ -111,10 +131,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   const int variant = p.beta_nonzero ? 2 : (p.streaming ? 1 : 0);
   ttcb::KernelRef k = ttcb::pick_kernel(p.ta, p.tb, kernel, va, vb, variant);
   if (!k.fn) return na_fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
-  if (p.smem_async + (int)ttcb::kAsyncStaticSmem > 48 * 1024) {
-    e = cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_async);
-    if (e != cudaSuccess) return na_cuda(e, "cudaFuncSetAttribute");
-  }
+  if (ttcb::needs_large_smem(p.smem_async)) ttcb::allow_large_smem(k.func);
   int sms = 0, per_sm = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
     return na_cuda(e, "cudaDeviceGetAttribute");
@@ -133,12 +150,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
       p.dev_desc = nullptr;
       return na_fail(TTCB_ERR_DTYPE, "no ragged-tile kernel for this type pair");
     }
-    if (p.smem_ragged + (int)ttcb::kAsyncStaticSmem > 48 * 1024 &&
-        (e = cudaFuncSetAttribute(kr.func, cudaFuncAttributeMaxDynamicSharedMemorySize, p.smem_ragged)) !=
-            cudaSuccess) {
-      p.dev_desc = nullptr;
-      return na_cuda(e, "cudaFuncSetAttribute");
-    }
+    if (ttcb::needs_large_smem(p.smem_ragged)) ttcb::allow_large_smem(kr.func);
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr.func, ttcb::kThreads, p.smem_ragged)) ==
         cudaSuccess) {
       const int64_t rw = (int64_t)td->nrag0 + td->nrag1, rres = (int64_t)std::max(per_sm, 1) * sms;
@@ -149,4 +161,11 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   p.dev_desc = nullptr;  // the scratch belongs to the library, not to this stack plan
   if (e != cudaSuccess) return na_cuda(e, "kernel launch");
   return TTCB_OK;
+}
+
+// Test hook (testing.h): lowers the largest descriptor the entry point accepts (0 restores the
+// scratch size), so that a CPU test reaches the rejection with an ordinary problem. No CUDA call.
+extern "C" size_t ttcb_test_noalloc_limit(size_t bytes) {
+  g_noalloc_limit = (bytes == 0 || bytes > kNoAllocScratchBytes) ? kNoAllocScratchBytes : bytes;
+  return kNoAllocScratchBytes;
 }

@@ -976,6 +976,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"ngrid\":" << t->ngrid << ",\"nblocked\":" << t->nblocked << ",\"pad\":" << t->pad
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
+      << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
       << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";

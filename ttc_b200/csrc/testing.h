@@ -24,6 +24,9 @@ size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, con
                              size_t len);
 // The boxes a plan's ragged tiles are moved as (edge plans), host-only: a JSON array of
 // {"rank","perm","size","lda","ldb","offA","offB"}; returns the length needed, 0 on failure.
+// Lowers the largest descriptor ttcb_transpose_noalloc accepts to `bytes` (0 restores the full
+// scratch size) and returns the scratch size. Makes no CUDA call.
+size_t ttcb_test_noalloc_limit(size_t bytes);
 size_t ttcb_test_plan_edges(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
                             int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len);
 }

@@ -231,6 +231,7 @@ def generateTransposition(ttcArgs: TTCargs):
     sizeOld, permOld, ldaOld, ldbOld = map(copy.deepcopy, (a.size, a.idxPerm, a.lda, a.ldb))
     fsize, fperm, flda, fldb = list(a.size), list(a.idxPerm), list(a.lda), list(a.ldb)
     ttc_util.fuseIndices(fsize, fperm, [], flda, fldb)
+    flda, fldb = ttc_util.denseLeadingDims(fsize, fperm, flda, fldb)
     if len(fsize) != len(sizeOld) and not a.silent:
         print("Permutation and Size _before_ index-fusion: ", permOld, sizeOld, ldaOld, ldbOld)
         print("Permutation and Size _after_ index-fusion: ", fperm, fsize, flda, fldb)

@@ -125,11 +125,14 @@ def getCostLoop(loopPerm, perm, size) -> float:
 
 def fuseIndices(size, perm, loopPermutations, lda, ldb):
     """In-place index fusion with TTC's semantics (ttc_util.py:214-276): runs of A-dims that stay
-    consecutive in B and are unpadded become one dimension; loop orders are renumbered."""
+    consecutive in B and are unpadded become one dimension; loop orders are renumbered. An empty
+    lda (ldb) means dense: the fusion then works on a local dense copy and the caller's list stays
+    empty, as in TTC, whose generators fill the dense defaults from the fused sizes
+    (GPUtransposeGenerator.py:87-94)."""
     if len(lda) == 0:
-        lda[:] = list(size)
+        lda = list(size)
     if len(ldb) == 0:
-        ldb[:] = [size[p] for p in perm]
+        ldb = [size[p] for p in perm]
     idx = list(range(len(size)))
     i = 0
     while i < len(idx):
@@ -162,6 +165,12 @@ def fuseIndices(size, perm, loopPermutations, lda, ldb):
         for k in range(len(loopOrder)):
             loopOrder[k] -= diff
         loopOrder[:] = [x for x in loopOrder if x >= 0]
+
+
+def denseLeadingDims(size, perm, lda, ldb):
+    """lda/ldb with TTC's dense defaults filled in (lda = size, ldb[j] = size[perm[j]]) where the
+    caller left them empty (GPUtransposeGenerator.py:87-94)."""
+    return (list(lda) if len(lda) else list(size)), (list(ldb) if len(ldb) else [size[p] for p in perm])
 
 
 def streamingStoresApplicable(ldb, size, perm, beta, alignmentRequirementBytes, floatSizeBytes, useStreamingStores):
