@@ -66,14 +66,24 @@ typedef struct {
   int32_t blocks;        /* CTAs launched (persistent grid); 0 = all tiles / occupancy bound  */
   int32_t loop_order;    /* raster of the tile grid: 0 = planner's choice (B-major when B's runs
                             are under 256 bytes and B exceeds 64 MiB, else A-major), 1 = B-major,
-                            2 = reverse A, 3 = A-major                                          */
+                            2 = reverse A, 3 = A-major, 4 = the explicit order in raster_lo/hi  */
   int32_t streaming;     /* 0 = default (streaming stores when beta == 0), 1 = on, -1 = off     */
   int32_t tile_variant;  /* tile kernel: 0 auto, 1 table-driven, 2 register-resident prefetch,
                             3 staged asynchronous copies                                        */
   int32_t ragged;        /* staged tile kernel's ragged tiles (last blocks of dimensions that
                             the tile does not divide): 0 = planned as transpositions of their
                             own and moved by the staged kernel, 1 = element-wise kernel         */
-  int32_t reserved[7];
+  /* loop_order == 4: TTC's loop order (--loopPerm, GPUtransposeGenerator.py:203-230), the caller's
+     dimensions from the fastest-varying tile index to the slowest, packed 4 bits per dimension as
+     (dimension + 1): dimensions 0..7 of the order in raster_lo (first in the low bits), 8..9 in
+     raster_hi. Dimensions that index fused groups are ordered by their first appearance; those the
+     tile covers whole do not step the grid. Every dimension must appear exactly once. */
+  int32_t raster_lo;
+  int32_t raster_hi;
+  int32_t stages;        /* staged tile kernel: shared-memory ring stages (3..7, stages - 2 tiles of
+                            copies in flight); 0 = planner's choice (4 while four CTAs fit an SM,
+                            else 3)                                                             */
+  int32_t reserved[4];
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

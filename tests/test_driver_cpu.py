@@ -114,3 +114,18 @@ def test_main_reports_errors_without_exiting(capsys):
     assert ttc.main(["--perm=1,0", "--size=3,4", "--lda=2,4", "--architecture=cuda"]) == 1
     out = capsys.readouterr().out
     assert "leading dimension of A" in out
+
+
+def test_loop_perm_flags_become_explicit_rasters():
+    """--loopPerm restricts the search to the given loop orders, each kept as given (the explicit
+    raster, ttcb_tuning loop_order 4); without it, TTC's cost-ranked orders join the presets."""
+    from ttc_b200.autotune import Problem, candidate_tunings
+    a = ttc.parse_args(["--perm=1,0,2", "--size=1000,768,16", "--loopPerm=2,0,1-1,2,0"])
+    space = ttc._tunings_from_args(a, "s")
+    assert space["loop_order"] == [] and space["rasters"] == [[2, 0, 1], [1, 2, 0]]
+    cands = candidate_tunings(Problem([1, 0, 2], [1000, 768, 16], "s"), 1000, space)
+    rasters = {tuple(t["raster"]) for t in cands if "raster" in t}
+    assert rasters == {(2, 0, 1), (1, 2, 0)}
+    assert all("raster" in t for t in cands)
+    b = ttc.parse_args(["--perm=1,0,2", "--size=1000,768,16"])
+    assert ttc._tunings_from_args(b, "s")["rasters"] == ("ttc", 2)

@@ -112,6 +112,15 @@ def test_schedule_knobs_do_not_change_results(tuning):
                 raise
 
 
+@pytest.mark.parametrize("order", [[0, 1, 2], [0, 2, 1], [1, 0, 2], [1, 2, 0], [2, 0, 1], [2, 1, 0]])
+def test_every_explicit_loop_order(order):
+    """TTC's --loopPerm as the tile grid's raster: each of the six orders of a rank-3 problem whose
+    tile leaves every dimension in the grid, with ragged blocks, for beta = 0 and beta != 0."""
+    for dtype, beta in (("s", 0.0), ("d", -0.5)):
+        desc = check_case([1, 0, 2], [301, 263, 7], dtype, 1.5, beta, tuning={"raster": order})
+        assert desc["loop_order"] == 4
+
+
 @pytest.mark.parametrize("offset", [1, 2, 3])
 def test_misaligned_pointers_fall_back_to_narrow_accesses(offset):
     check_case([1, 0, 2], [64, 96, 3], "s", 1.0, 0.5, offset=offset)

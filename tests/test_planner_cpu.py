@@ -306,3 +306,68 @@ def test_candidate_rasters_name_each_order_once():
         orders = {tu.get("loop_order", 0) for tu, d in cands if d["kernel"] == "tile" and d["loop_order"] == chosen}
         assert chosen not in orders and other in orders and 0 in orders and 2 in orders, (orders, chosen)
         assert len({json.dumps(tu, sort_keys=True) for tu, _ in cands}) == len(cands)
+
+
+def test_explicit_loop_orders_become_the_tile_grid_raster():
+    """TTC's --loopPerm (GPUtransposeGenerator.py:203-230; blockIdx decoded fastest first,
+    CUDAtranspose.py:737-779) as an explicit raster: for the README shape, whose tile leaves all three
+    dimensions in the grid, every one of the six orders yields exactly that raster; fused groups take
+    the place of their first member, dimensions the tile covers whole leave the grid, and orders that
+    are not permutations are refused."""
+    import itertools
+    from ttc_b200 import TTCError
+    from ttc_b200.core import plan_host_json
+    for order in itertools.permutations(range(3)):
+        d = plan_host_json([1, 0, 2], [1000, 768, 16], "s", True, tuning={"raster": list(order)})
+        assert d["loop_order"] == 4 and d["raster"] == list(order), (order, d["raster"], d["tile"]["ext"])
+    # an extent-1 dimension (here 1) is dropped by the fusion, but the order still lists it
+    d = plan_host_json([2, 0, 3, 1], [64, 1, 48, 40], "s", False, tuning={"raster": [3, 1, 2, 0]})
+    fused_of = {0: 0, 2: 1, 3: 2}
+    want = [fused_of[x] for x in (3, 2, 0)]
+    ext = d["tile"]["ext"]
+    want = [w for w in want if not (ext[w] and ext[w] == d["fused"]["size"][w])]
+    assert d["raster"] == want, (d["raster"], want, ext)
+    for bad in ([0, 0, 1], [0, 1], [0, 1, 3]):
+        with pytest.raises(TTCError):
+            plan_host_json([1, 0, 2], [10, 20, 30], "s", False, tuning={"raster": bad})
+
+
+def test_search_adds_ttc_ranked_loop_orders():
+    """With TTC's ranking switched on, the search adds up to two explicit loop orders per tile shape,
+    taken cheapest first by ttc_util.getCostLoop, and only those whose raster no preset order gives."""
+    from ttc_b200.autotune import (Problem, candidate_tunings, grid_raster, knob_space, preset_order,
+                                   ranked_loop_orders, fused_groups)
+    from ttc_b200.ttc_util import getCostLoop
+    p = Problem([4, 2, 1, 3, 0], [39, 4, 7, 153, 314], "s", 1.0, 0.0)
+    fperm, fsize, groups = fused_groups(p)
+    ranked = ranked_loop_orders(p, 10)
+    costs = []
+    for o in ranked:
+        fo = []
+        for dd in o:
+            fd = next(i for i, g in enumerate(groups) if dd in g)
+            if fd not in fo:
+                fo.append(fd)
+        costs.append(getCostLoop(fo, fperm, fsize))
+    assert costs == sorted(costs)
+    cands = candidate_tunings(p, 500, knob_space("s", ttc_orders=2), with_desc=True)
+    by_shape = {}
+    for tu, d in cands:
+        if d["kernel"] != "tile":
+            continue
+        key = json.dumps({k: v for k, v in tu.items() if k in ("tile_elems", "run_bytes")}, sort_keys=True)
+        by_shape.setdefault(key, (d, []))[1].append(tu)
+    assert any("raster" in tu for _, tus in by_shape.values() for tu in tus)
+    for d, tus in by_shape.values():
+        rasters = []
+        for tu in tus:
+            if "raster" in tu:
+                fo = []
+                for dd in tu["raster"]:
+                    fd = next(i for i, g in enumerate(groups) if dd in g)
+                    if fd not in fo:
+                        fo.append(fd)
+                rasters.append(grid_raster(d, fo))
+            else:
+                rasters.append(grid_raster(d, preset_order(d, tu.get("loop_order", 0))))
+        assert len(set(rasters)) == len(set(json.dumps(tu, sort_keys=True) for tu in tus if not tu.get("blocks")))

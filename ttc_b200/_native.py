@@ -31,21 +31,57 @@ class TTCError(RuntimeError):
         super().__init__(f"[TTC] ERROR ({self.code}): {message}")
 
 
+def pack_raster(order) -> tuple[int, int]:
+    """An explicit loop order (the caller's dimensions, fastest-varying first) in ttcb_tuning's
+    raster_lo / raster_hi encoding: 4 bits per position, holding dimension + 1."""
+    order = [int(d) for d in order]
+    if sorted(order) != list(range(len(order))) or not 1 <= len(order) <= MAX_RANK:
+        raise TTCError(3, f"loop order {order} is not a permutation of the dimensions")
+    lo = hi = 0
+    for k, d in enumerate(order):
+        if k < 8:
+            lo |= (d + 1) << (4 * k)
+        else:
+            hi |= (d + 1) << (4 * (k - 8))
+    return ctypes.c_int32(lo).value, hi
+
+
+def unpack_raster(lo: int, hi: int) -> list:
+    out = []
+    for k in range(MAX_RANK):
+        w = (lo & 0xFFFFFFFF) if k < 8 else hi
+        d = (w >> (4 * (k % 8))) & 0xF
+        if d == 0:
+            break
+        out.append(d - 1)
+    return out
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("tile_elems", ctypes.c_int32), ("run_bytes", ctypes.c_int32),
                 ("vec", ctypes.c_int32), ("blocks", ctypes.c_int32), ("loop_order", ctypes.c_int32),
                 ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("ragged", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("raster_lo", ctypes.c_int32), ("raster_hi", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":
+        """Knobs by name; `raster=[d0, d1, ...]` (the caller's dimensions, fastest first) sets an
+        explicit loop order (loop_order 4)."""
         t = cls()
         for k, v in kw.items():
-            setattr(t, k, int(v))
+            if k == "raster":
+                t.raster_lo, t.raster_hi = pack_raster(v)
+                t.loop_order = 4
+            else:
+                setattr(t, k, int(v))
         return t
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "raster_lo", "raster_hi")}
+        if self.loop_order == 4:
+            d["raster"] = unpack_raster(self.raster_lo, self.raster_hi)
+        return d
 
 
 _lib = None

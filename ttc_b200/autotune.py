@@ -62,10 +62,14 @@ class Result:
     ok: bool = True
 
 
-def knob_space(dtype: str) -> dict:
+def knob_space(dtype: str, ttc_orders: int = 0) -> dict:
+    """The schedule knobs the search crosses. `ttc_orders` > 0 adds, per tile shape, up to that many
+    explicit loop orders from TTC's own ranking (see ranked_loop_orders) whose raster differs from
+    the preset orders'."""
     ta, _ = split_dtype(dtype)
     base = 16384 // ELEM_BYTES[ta]
     return {
+        "rasters": ("ttc", ttc_orders) if ttc_orders else [],
         "tile_elems": [0, base // 4, base // 2, base * 2],
         "run_bytes": [0, 128, 256, 512, 1024, 2048],
         # the register-prefetch (2) and table-driven (1) tile kernels were the fastest schedule for 12
@@ -75,6 +79,68 @@ def knob_space(dtype: str) -> dict:
         "loop_order": [0, 1, 2, 3],
         "blocks": [0, 2 * SMS, 3 * SMS],
     }
+
+
+def fused_groups(p: Problem):
+    """The library's index fusion of a problem (host only): (fused perm, fused sizes, groups), where
+    groups[i] lists the caller's dimensions of fused dimension i in A order; extent-1 dimensions are
+    in no group."""
+    from .core import fuse
+    la = p.lda or p.size
+    lb = p.ldb or [p.size[q] for q in p.perm]
+    r = len(p.size)
+    sA, sBp = [1] * r, [1] * r
+    for i in range(1, r):
+        sA[i] = sA[i - 1] * la[i - 1]
+        sBp[i] = sBp[i - 1] * lb[i - 1]
+    sB = [0] * r
+    for j, q in enumerate(p.perm):
+        sB[q] = sBp[j]
+    fperm, fsize, _, _ = fuse(p.perm, p.size, sA, sB)
+    groups, cur = [], []
+    dims = [d for d in range(r) if p.size[d] != 1]
+    k = 0
+    for fs in fsize:
+        prod, cur = 1, []
+        while k < len(dims) and prod < fs:
+            prod *= p.size[dims[k]]
+            cur.append(dims[k])
+            k += 1
+        groups.append(cur)
+    return fperm, fsize, groups
+
+
+def ranked_loop_orders(p: Problem, limit: int) -> list[list[int]]:
+    """TTC's loop-order heuristic: every order of the fused dimensions ranked by
+    ttc_util.getCostLoop, cheapest first, the first `limit` kept (GPUtransposeGenerator.py:203-230,
+    ttc_util.py:167-209), each written as an order of the caller's dimensions (extent-1 dimensions
+    last) for ttcb_tuning's explicit raster. Fused problems beyond rank 7 are not enumerated."""
+    from .ttc_util import getCostLoop
+    fperm, fsize, groups = fused_groups(p)
+    if len(fsize) > 7 or limit <= 0:
+        return []
+    ranked = sorted(itertools.permutations(range(len(fsize))), key=lambda lp: getCostLoop(lp, fperm, fsize))
+    unit = [d for d in range(len(p.size)) if p.size[d] == 1]
+    return [[d for fd in lp for d in groups[fd]] + unit for lp in ranked[:limit]]
+
+
+def grid_raster(desc: dict, order_fused: list) -> tuple:
+    """The tile-grid raster (fused grid dimensions, fastest first) that an order of the fused
+    dimensions gives a tile plan: the dimensions the tile covers whole do not step the grid."""
+    fu, t = desc["fused"], desc.get("tile") or {}
+    ext = t.get("ext") or [0] * fu["rank"]
+    return tuple(d for d in order_fused if not (ext[d] and ext[d] == fu["size"][d]))
+
+
+def preset_order(desc: dict, loop_order: int) -> list:
+    """The fused-dimension order of a preset loop_order value (0 resolves to the planner's choice)."""
+    fu = desc["fused"]
+    lo = loop_order or desc.get("loop_order", 3)
+    if lo == 1:
+        return list(fu["perm"])
+    if lo == 2:
+        return list(range(fu["rank"]))[::-1]
+    return list(range(fu["rank"]))
 
 
 def plan_signature(desc: dict) -> tuple:
@@ -109,18 +175,46 @@ def candidate_tunings(p: Problem, max_impl: int = 200, space: Optional[dict] = N
     (GPUtransposeGenerator.py:220-230); here the tile shapes are ordered by the planner's estimate
     and taken round-robin, so every shape gets its default schedule before any gets a second one."""
     space = space or knob_space(p.dtype)
+    rasters = space.get("rasters") or []
+    explicit = []  # explicit loop orders (the caller's dimensions), TTC-ranked or given
+    if isinstance(rasters, tuple) and rasters[0] == "ttc":
+        explicit = ranked_loop_orders(p, max(rasters[1], int(math.ceil(math.sqrt(max(max_impl, 1))))))
+        keep = rasters[1]
+    else:
+        explicit, keep = [list(r) for r in rasters], len(rasters)
+    fused = fused_groups(p)[2] if explicit else None
     lists = []
     for shape_tu, desc in tile_shapes(p, space):
         if desc["kernel"] == "row":
             combos = [dict(shape_tu, blocks=b) if b else dict(shape_tu) for b in space["blocks"]]
         else:
+            # the planner's raster choice (0) stands in for the explicit order it resolves to; an
+            # explicit order joins only when its raster is one no earlier order gives
+            orders, seen = [], set()
+            for lo in space["loop_order"]:
+                g = grid_raster(desc, preset_order(desc, lo))
+                if g not in seen:
+                    seen.add(g)
+                    orders.append({"loop_order": lo} if lo else {})
+            added = 0
+            for order in explicit:
+                if added >= keep:
+                    break
+                fo = []
+                for d in order:
+                    fd = next((i for i, grp in enumerate(fused) if d in grp), None)
+                    if fd is not None and fd not in fo:
+                        fo.append(fd)
+                g = grid_raster(desc, fo)
+                if g not in seen:
+                    seen.add(g)
+                    orders.append({"raster": list(order)})
+                    added += 1
             combos = []
-            # the planner's raster choice (0) stands in for the explicit order it resolves to
-            orders = [lo for lo in space["loop_order"]
-                      if not (lo and 0 in space["loop_order"] and lo == desc.get("loop_order"))]
             for v, lo, b in itertools.product(space["tile_variant"], orders, space["blocks"]):
                 tu = dict(shape_tu)
-                for k, val in (("tile_variant", v), ("loop_order", lo), ("blocks", b)):
+                tu.update(lo)
+                for k, val in (("tile_variant", v), ("blocks", b)):
                     if val:
                         tu[k] = val
                 combos.append(tu)

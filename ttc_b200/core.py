@@ -153,7 +153,8 @@ def transpose(A, B, perm: Sequence[int], size: Optional[Sequence[int]] = None, a
     if tb != dtype:
         dtype = dtype + tb
     key = (tuple(perm), tuple(size), dtype, complex(beta) != 0, tuple(lda or ()), tuple(ldb or ()),
-           tuple(sorted((tuning or {}).items())), A.device.index)
+           tuple(sorted((k, tuple(v) if isinstance(v, list) else v) for k, v in (tuning or {}).items())),
+           A.device.index)
     plan = _plan_cache.get(key)
     if plan is None:
         plan = Plan(perm, size, dtype, complex(beta) != 0, lda, ldb, tuning)

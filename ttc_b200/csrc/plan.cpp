@@ -49,11 +49,12 @@ void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA
   struct Grp {
     int64_t n, sA, sB;
     int id;
+    unsigned members;  // the caller's dimensions in this group (bit mask)
   };
   std::vector<Grp> a;      // groups in A order
   std::vector<int> border; // group ids in B order
   for (int i = 0; i < rank; ++i)
-    if (n[i] != 1) a.push_back({n[i], sA[i], sB[i], i});
+    if (n[i] != 1) a.push_back({n[i], sA[i], sB[i], i, 1u << i});
   for (int j = 0; j < rank; ++j)
     if (n[perm[j]] != 1) border.push_back(perm[j]);
 
@@ -66,6 +67,7 @@ void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA
       size_t pg = std::find(border.begin(), border.end(), g.id) - border.begin();
       if (pg + 1 < border.size() && border[pg + 1] == h.id && h.sA == g.sA * g.n && h.sB == g.sB * g.n) {
         a[k].n *= h.n;
+        a[k].members |= h.members;
         border.erase(border.begin() + pg + 1);
         a.erase(a.begin() + k + 1);
         changed = true;
@@ -74,6 +76,7 @@ void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA
     }
   }
   out = FusedProblem();
+  for (int i = 0; i < rank; ++i) out.fused_of[i] = -1;
   if (a.empty()) {
     out.rank = 1;
     out.perm[0] = 0;
@@ -83,6 +86,9 @@ void fuse_problem(int rank, const int* perm, const int64_t* n, const int64_t* sA
     return;
   }
   out.rank = (int)a.size();
+  for (int i = 0; i < out.rank; ++i)
+    for (int d = 0; d < rank; ++d)
+      if (a[i].members & (1u << d)) out.fused_of[d] = i;
   for (int i = 0; i < out.rank; ++i) {
     out.n[i] = a[i].n;
     out.sA[i] = a[i].sA;
@@ -589,6 +595,18 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     for (int j = 0; j < f.rank; ++j) gdims.push_back(f.perm[j]);
   } else if (p->loop_order == 2) {
     for (int i = f.rank - 1; i >= 0; --i) gdims.push_back(i);
+  } else if (p->loop_order == 4) {
+    // the caller's loop order: each fused dimension at the first appearance of one of its members
+    int order[TTCB_MAXR];
+    unpack_raster(p->tuning, p->rank, order);
+    bool seen[TTCB_MAXR] = {false};
+    for (int k = 0; k < p->rank; ++k) {
+      const int fd = f.fused_of[order[k]];
+      if (fd >= 0 && !seen[fd]) {
+        seen[fd] = true;
+        gdims.push_back(fd);
+      }
+    }
   } else {
     for (int i = 0; i < f.rank; ++i) gdims.push_back(i);
   }
@@ -619,6 +637,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   }
   td.ngrid = ng;
   td.nblocked = nb;
+  p->nraster = ng;
+  for (int k = 0; k < ng; ++k) p->raster[k] = gdim_of[k];
   td.ntiles = (int32_t)ntiles;
   td.rag_a = td.rag_b = -1;
   for (int k = 0; k < ng; ++k)
@@ -676,6 +696,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     // each), else three (one tile in flight); deeper rings (up to ttcb::kMaxStages) measured
     // slower on the sweep, with four CTAs or with fewer
     td.nstages = smem_for(4) <= 56 * 1024 ? 4 : 3;
+    if (p->tuning.stages >= 3 && p->tuning.stages <= ttcb::kMaxStages) td.nstages = p->tuning.stages;
     td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
@@ -746,6 +767,23 @@ static ttcb_status build_row_desc(ttcb_plan* p, std::string& err) {
   return TTCB_OK;
 }
 
+bool unpack_raster(const ttcb_tuning& tu, int rank, int* order) {
+  bool seen[TTCB_MAXR] = {false};
+  for (int k = 0; k < rank; ++k) {
+    const uint32_t w = (uint32_t)(k < 8 ? tu.raster_lo : tu.raster_hi);
+    const int d = (int)((w >> (4 * (k % 8))) & 0xfu) - 1;
+    if (d < 0 || d >= rank || seen[d]) return false;
+    seen[d] = true;
+    order[k] = d;
+  }
+  // nothing may follow the last dimension
+  for (int k = rank; k < 10; ++k) {
+    const uint32_t w = (uint32_t)(k < 8 ? tu.raster_lo : tu.raster_hi);
+    if ((w >> (4 * (k % 8))) & 0xfu) return false;
+  }
+  return true;
+}
+
 // ------------------------------------------------------------------------------------------------
 ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   const int r = p->rank;
@@ -813,6 +851,17 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   p->streaming = (p->tuning.streaming == 1) || (p->tuning.streaming == 0 && !p->beta_nonzero);
   if (p->beta_nonzero) p->streaming = false;
   p->loop_order = p->tuning.loop_order ? p->tuning.loop_order : 3;  // the tile planner may choose
+  if (p->tuning.loop_order < 0 || p->tuning.loop_order > 4) {
+    err = "loop_order must be in [0, 4]";
+    return TTCB_ERR_INVALID_ARG;
+  }
+  if (p->tuning.loop_order == 4) {
+    int order[TTCB_MAXR];
+    if (!unpack_raster(p->tuning, r, order)) {
+      err = "the loop order (raster_lo/raster_hi) is not a permutation of the dimensions";
+      return TTCB_ERR_BAD_PERM;
+    }
+  }
   if (p->empty) {
     p->kernel = 0;
     p->f.rank = 0;
@@ -967,7 +1016,10 @@ std::string plan_describe_json(const ttcb_plan* p) {
   o << "]}";
   o << ",\"kernel\":\"" << (p->kernel == TTCB_KERNEL_TILE ? "tile" : p->kernel == TTCB_KERNEL_ROW ? "row" : "none")
     << "\",\"vecA\":" << p->vecA << ",\"vecB\":" << p->vecB << ",\"blocks\":" << p->blocks
-    << ",\"streaming\":" << (p->streaming ? 1 : 0) << ",\"loop_order\":" << p->loop_order
+    << ",\"streaming\":" << (p->streaming ? 1 : 0) << ",\"loop_order\":" << p->loop_order;
+  o << ",\"raster\":[";
+  for (int k = 0; k < p->nraster; ++k) o << (k ? "," : "") << p->raster[k];
+  o << "]"
     << ",\"tile_variant\":" << p->tuning.tile_variant
     << ",\"smem\":" << p->smem_bytes << ",\"est_cost\":" << p->est_cost;
   if (p->kernel == TTCB_KERNEL_TILE && !p->host_desc.empty()) {

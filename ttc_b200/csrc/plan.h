@@ -14,6 +14,8 @@ struct FusedProblem {
   int64_t sB[TTCB_MAXR] = {0};   // B stride of A-dim i
   int64_t oA = 0, oB = 0;        // offsets (elements) of A and B from a 16-byte boundary; only their
                                  // alignment matters (nonzero for the edge plans of another plan)
+  int fused_of[TTCB_MAXR] = {0}; // the caller's dimension i belongs to fused dimension fused_of[i]
+                                 // (-1: an extent-1 dimension, dropped)
 };
 
 // A box of a tile plan's ragged tiles (the last block of one ragged dimension; with two ragged
@@ -50,6 +52,8 @@ struct ttcb_plan {
   int blocks = 0;         // CTAs launched
   bool streaming = false;
   int loop_order = 0;
+  int raster[TTCB_MAXR] = {0};  // grid dimensions (fused) from the fastest-varying to the slowest
+  int nraster = 0;
   double est_cost = 0.0;  // planner's cost estimate (bytes-equivalent per element)
 
   // descriptor (host copy + device copy)
@@ -95,6 +99,10 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err);
 // and reuses them for further tunings of the same problem (used to plan many candidates quickly).
 void plan_tile_cache_begin();
 void plan_tile_cache_end();
+
+// Decodes an explicit loop order (ttcb_tuning::raster_lo/hi) into `order` (the caller's dimensions,
+// fastest first); false unless it is a permutation of 0..rank-1.
+bool unpack_raster(const ttcb_tuning& tu, int rank, int* order);
 
 // Fusion of adjacent dimensions that stay adjacent in B (exposed for tests through the C ABI of
 // the test helper in abi.cu).

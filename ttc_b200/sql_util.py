@@ -167,7 +167,7 @@ def insert(path: str, size, perm, floatTypeA, floatTypeB, alpha, beta, architect
         mid = int(cur.lastrowid)
         for v in variants:
             t = v["tuning"]
-            loop = [t.get("loop_order", 0)]
+            loop = list(t["raster"]) if t.get("raster") else [t.get("loop_order", 0)]
             lid = _get_or_insert(cur, "loopOrder", "loopOrder_id", "idx", loop)
             cur.execute("""INSERT INTO variant (blockA, blockB, prefetchDistance, bandwidth, time, tlbMisses,
                            l2misses, rankLoopOrder, rankBlocking, measurement_id, loopOrder_id, tuning)

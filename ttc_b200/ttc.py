@@ -110,7 +110,10 @@ def emit_shim(ttcArgs, file_name: str, func: str, tuning: dict, size, perm, lda,
         h += f"{alias};\n"
     h += "#endif\n"
     rank = len(size)
-    fields = " ".join(f"t.{k} = {int(v)};" for k, v in sorted(tuning.items()))
+    from ._native import Tuning
+    packed = Tuning.make(**tuning)  # an explicit loop order travels as raster_lo/raster_hi
+    fields = " ".join(f"t.{k} = {int(getattr(packed, k))};" for k, _ in Tuning._fields_
+                      if k != "reserved" and int(getattr(packed, k)) != 0)
     a_val = f"{SCALAR[ta]} a[2] = {{alpha, 0}};" if "complex" in ta else f"{SCALAR[ta]} a[1] = {{alpha}};"
     b_val = (f"{SCALAR[tb]} b[2] = {{beta, 0}};" if "complex" in tb else f"{SCALAR[tb]} b[1] = {{beta}};") \
         if beta else f"{SCALAR[tb]}* b = 0;"
@@ -190,17 +193,12 @@ def _tunings_from_args(a: TTCargs, dtype: str):
         space["tile_elems"] = sorted({int(bA) * int(bB) for bA, bB in a.blockings})
         space["run_bytes"] = sorted({int(bA) * ea for bA, _ in a.blockings})
     if a.loopPermutations:
-        orders = set()
-        rank = len(a.idxPerm)
-        for lp in a.loopPermutations:
-            lp = list(lp)
-            if lp == sorted(lp):
-                orders.add(3)
-            elif lp == sorted(lp, reverse=True):
-                orders.add(2)
-            else:
-                orders.add(1)
-        space["loop_order"] = sorted(orders)
+        # each given loop order becomes the tile grid's raster, as given (no preset stands in)
+        space["loop_order"] = []
+        space["rasters"] = [list(lp) for lp in a.loopPermutations]
+    else:
+        # TTC ranks every loop order with its cost heuristic and keeps the cheapest
+        space["rasters"] = ("ttc", 2)
     return space
 
 
