@@ -491,6 +491,17 @@ def run_sweep(args, rank, world, local):
     cases = wl.sweep_cases(rank_seed(args.seed, rank))[: args.cases]
     tmap = {"s": torch.float32, "d": torch.float64}
 
+    # the learned selector needs its trained model; without one the planner's defaults are timed
+    # and the line says so
+    schedule_note = None
+    if args.schedule == "learned":
+        try:
+            from ttc_b200 import cost_model
+            cost_model.load_default()
+        except Exception as ex:
+            args.schedule = "default"
+            schedule_note = f"learned model unavailable ({type(ex).__name__}: {ex}); planner defaults timed"
+
     # resident inputs, seeded on the device
     gen = torch.Generator(device=dev)
     items = []
@@ -599,7 +610,8 @@ def run_sweep(args, rank, world, local):
 
     extras = {}
     if world == 1 and not args.no_extras:
-        for name, fn in (("configs", lambda: configs_summary(args)), ("batched", lambda: batched_summary(args)),
+        for name, fn in (("reference_gpu", lambda: reference_gpu_summary(args)),
+                         ("configs", lambda: configs_summary(args)), ("batched", lambda: batched_summary(args)),
                          ("selector", lambda: selector_summary(args))):
             try:
                 extras[name] = fn()
@@ -613,8 +625,9 @@ def run_sweep(args, rank, world, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded uniform[-1,1])",
                 "pct_of_hbm_peak": round(100 * value / world / peak, 2),
                 "config": sweep_config(len(cases), bytes_per_step, world),
-                "schedules": ("learned selector (top-1; timed against the planner default when its confidence "
-                              "< 0.1)" if args.schedule == "learned" else "planner default"),
+                "schedules": schedule_note or ("learned selector (top-1; timed against the planner default when "
+                                               "its confidence < 0.1)" if args.schedule == "learned"
+                                               else "planner default"),
                 "schedule_seconds": round(t_sel, 1),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches_per_step * args.steps, **extras}
@@ -725,47 +738,73 @@ def batched_summary(args):
             "mismatches_vs_per_call": mismatches, "steps": 10}
 
 
+def reference_gpu_summary(args):
+    """TTC's own CUDA kernels on this GPU (oracle/_ref/libttc_ref_cuda.so: the first variants of TTC's
+    CUDA generator's own order per case, compiled for sm_100a) over the 64-case sweep, on the same
+    seeded inputs: per case every built variant is called through TTC's generated wrapper (per-call
+    cudaMalloc/cudaMemcpy of the sizes, launch, cudaDeviceSynchronize, cudaFree; CUDAtranspose.py:
+    395-429 in the TTC project) and the fastest kept, as TTC's search would. Kernel-only time is the
+    device time of TTC's kernels from CUDA's activity records (torch.profiler, min of 3 calls);
+    wrapper time is the host wall time of the synchronous call."""
+    import torch
+    import ttc_b200.workloads as wl
+    from oracle import cuda_ref
+    from torch.profiler import ProfilerActivity, profile
+    ref = cuda_ref.available()
+    if ref is None:
+        return {"unavailable": "TTC's CUDA kernels were not built (oracle/make_ref_gpu.py needs the TTC sources)"}
+    tmap = {"s": torch.float32, "d": torch.float64}
+    cases = [c for c in wl.sweep_cases(args.seed)[: args.cases] if ref.covers(c)]
+    tot_bytes, t_kernel, t_wrap, chosen = 0, 0.0, 0.0, []
+    gen = torch.Generator(device="cuda")
+    for c in cases:
+        n = math.prod(c["size"])
+        gen.manual_seed(c["seed"])
+        A = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen).mul_(2).sub_(1)
+        gen.manual_seed(c["seed"] + 1)
+        B = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen).mul_(2).sub_(1)
+        variants = ref.variants(c)
+        for j in range(len(variants)):  # warm every variant's module and launch path
+            ref.call(c, j, A.data_ptr(), B.data_ptr())
+        walls = []
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            for j in range(len(variants)):
+                w = float("inf")
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    ref.call(c, j, A.data_ptr(), B.data_ptr())
+                    w = min(w, time.perf_counter() - t0)
+                walls.append(w)
+        kern = [float("inf")] * len(variants)
+        for ev in prof.events():
+            if ev.device_type != torch.autograd.DeviceType.CUDA:
+                continue
+            for j, v in enumerate(variants):
+                if v["kernel"] in ev.name:
+                    kern[j] = min(kern[j], ev.device_time_total * 1e-6)
+        best = min(range(len(variants)), key=lambda j: kern[j])
+        tot_bytes += wl.case_bytes(c)
+        t_kernel += kern[best]
+        t_wrap += walls[best]
+        chosen.append(variants[best]["version"])
+        del A, B
+    torch.cuda.empty_cache()
+    m = ref.manifest
+    return {"cases": len(cases), "variants_per_case": m["variants_per_case"],
+            "kernel_GBps": round(tot_bytes / t_kernel / 1e9, 1), "wrapper_GBps": round(tot_bytes / t_wrap / 1e9, 1),
+            "chosen_versions": chosen, "nvcc": " ".join(m["nvcc_flags"]),
+            "note": ("TTC's CUDA generator (--maxImplementations 200 ordering), first variants per case compiled "
+                     "for sm_100a; fastest by kernel device time on this GPU")}
+
+
 def selector_summary(args):
     """The learned selector against a fresh measured search on held-out problems (the first
-    `--selector-cases` problems of the held-out seed, 1-256 MiB): per problem, every candidate is
-    timed (the exhaustive search), then the search's winner, the network's top-1 and the planner
-    default are re-timed alternately (so the winner loses the bias of being the maximum of noisy
-    timings); tuning time is the search's wall time against the selector's (planning, features,
-    inference, and its timed fallback when unsure)."""
+    `--selector-cases` problems of the held-out seed, 1-256 MiB): see cost_model.fresh_head_to_head."""
     import ttc_b200.workloads as wl
     from ttc_b200 import cost_model
-    from ttc_b200.autotune import Bench, Problem, measure, search
-    model = cost_model.load_default()
-    rows = []
-    for c in wl.learning_cases(cost_model.HELDOUT_SEED, args.selector_cases):
-        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
-        sr = search(p, max_impl=64, reps=3, verify=False)
-        sel_top1 = cost_model.select(p, confidence=0.0, model=model, verify=False, measure_choice=False)
-        sel = cost_model.select(p, model=model, verify=False, measure_choice=False)
-        top1 = sel_top1["candidates"][int(sel_top1["order"][0])][0]
-        chosen = min(sel["results"], key=lambda r: r.time_ms).tuning if sel["results"] else top1
-        picks = [sr["best"].tuning, top1, chosen, {}]
-        bench = Bench(p, seed=1)
-        best_ms = [float("inf")] * len(picks)
-        for rnd in range(2):
-            order = list(range(len(picks))) if rnd == 0 else list(reversed(range(len(picks))))
-            for i, r in zip(order, measure(p, [picks[i] for i in order], reps=5, verify=False, bench=bench)):
-                best_ms[i] = min(best_ms[i], r.time_ms)
-        del bench
-        rows.append({"search_s": sr["seconds"], "top1_s": sel_top1["seconds"], "sel_s": sel["seconds"],
-                     "top1": best_ms[0] / best_ms[1], "sel": best_ms[0] / best_ms[2], "dflt": best_ms[0] / best_ms[3],
-                     "fallback": bool(sel["fallback"])})
-    m = lambda k: float(np.mean([r[k] for r in rows]))
-    return {"problems": len(rows), "held_out_seed": cost_model.HELDOUT_SEED, "search_candidates": 64,
-            "top1_over_search": round(m("top1"), 4), "selector_over_search": round(m("sel"), 4),
-            "default_over_search": round(m("dflt"), 4),
-            "selector_within_5pct": round(float(np.mean([r["sel"] >= 0.95 for r in rows])), 4),
-            "fallbacks": int(sum(r["fallback"] for r in rows)),
-            "search_seconds_mean": round(m("search_s"), 3), "selector_seconds_mean": round(m("sel_s"), 4),
-            "top1_seconds_mean": round(m("top1_s"), 4),
-            "tuning_time_ratio_selector": round(m("search_s") / max(m("sel_s"), 1e-9), 1),
-            "tuning_time_ratio_top1": round(m("search_s") / max(m("top1_s"), 1e-9), 1),
-            "timing": "fresh: winner, top-1, selector choice and default re-timed alternately, best of 2x5 launches"}
+    out = cost_model.fresh_head_to_head(wl.learning_cases(cost_model.HELDOUT_SEED, args.selector_cases))
+    out["held_out_seed"] = cost_model.HELDOUT_SEED
+    return out
 
 
 # ------------------------------------------------------------------------------------------------

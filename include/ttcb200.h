@@ -81,9 +81,12 @@ typedef struct {
   int32_t raster_lo;
   int32_t raster_hi;
   int32_t stages;        /* staged tile kernel: shared-memory ring stages (3..7, stages - 2 tiles of
-                            copies in flight); 0 = planner's choice (4 while four CTAs fit an SM,
-                            else 3)                                                             */
-  int32_t reserved[4];
+                            copies in flight); 0 = planner's choice                             */
+  int32_t ctas_per_sm;   /* staged tile kernel: resident CTAs per SM (1..8, capped by what fits);
+                            0 = planner's choice. `blocks`, when set, takes precedence          */
+  int32_t round_robin;   /* staged tile kernel: 0 = CTAs claim tiles in order from a counter the
+                            plan owns, 1 = fixed round-robin order (tile blockIdx + k * CTAs)    */
+  int32_t reserved[2];
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;
@@ -107,6 +110,10 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
  * plan created with beta_nonzero == 0. */
 ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const void* alpha,
                            const void* beta, ttcb_stream_t stream);
+/* Calls with one plan may overlap on the GPU (several streams): its staged kernel takes the counter
+ * words it claims tiles from in turn from 64 slot pairs, so up to 64 launches of one plan can be in
+ * flight at once. A launch captured in a CUDA graph keeps its slot; replays of that graph must not
+ * overlap each other. */
 
 /* Allocation-free transposition, for callers that may not allocate device memory (their memory is
  * owned by an external pool, or cudaMalloc is forbidden where they run). It has no counterpart in

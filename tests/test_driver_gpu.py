@@ -116,8 +116,9 @@ int main(int argc, char** argv) {{
 
 
 def test_measured_search_verifies_and_ranks():
-    from ttc_b200.autotune import Problem, search
+    from ttc_b200.autotune import Problem, candidate_tunings, search
     p = Problem([2, 0, 1], [7, 3, 200001], "s", 1.5, -0.5)
     r = search(p, max_impl=16, reps=3)
-    assert r["candidates"] == 16 and all(x.ok for x in r["results"])
+    distinct = len(candidate_tunings(p, 1000))
+    assert r["candidates"] == min(16, distinct) >= 8 and all(x.ok for x in r["results"])
     assert r["best"].gbs == max(x.gbs for x in r["results"])

@@ -96,7 +96,8 @@ def test_padded_lda_ldb_and_complex_beta(dtype):
 
 TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"loop_order": 3}, {"blocks": 7}, {"tile_elems": 512},
            {"tile_elems": 8192}, {"run_bytes": 128}, {"run_bytes": 2048}, {"kernel": 1}, {"streaming": -1},
-           {"streaming": 1}]
+           {"streaming": 1}, {"round_robin": 1}, {"stages": 3}, {"stages": 7}, {"ctas_per_sm": 1},
+           {"stages": 6, "ctas_per_sm": 2}, {"round_robin": 1, "blocks": 5}]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS, ids=[str(t) for t in TUNINGS])
@@ -330,3 +331,37 @@ def test_edge_plans_random_ragged_problems(offset):
         desc = check_case(perm, size, dtype, 1.5, beta, lda, ldb, tuning, seed=100 + it, offset=offset)
         with_edges += bool(desc.get("edges"))
     assert with_edges >= 12, with_edges
+
+
+def test_claimed_tiles_with_concurrent_launches_and_slot_reuse():
+    """The staged kernel's tiles claimed from the plan's counters: one plan launched on four streams
+    at once (different counter slots), then 150 launches in a row on one stream (every slot used and
+    reset more than twice), each result bit for bit equal to the oracle's."""
+    import torch
+    from ttc_b200 import Plan
+    perm, size = [2, 0, 1], [67, 45, 311]
+    plan = Plan(perm, size, "s", True, tuning={"ctas_per_sm": 1})
+    assert plan.describe()["tile"]["async"] == 1
+    n = int(np.prod(size))
+    streams = [torch.cuda.Stream() for _ in range(4)]
+    ins, outs, wants = [], [], []
+    for k in range(4):
+        A, B = make_inputs(size, perm, "s", 300 + k)
+        wants.append(oracle.transpose(A, B.copy(), perm, size, 1.5, -0.5, dtype="s"))
+        ins.append(torch.from_numpy(A).cuda())
+        outs.append(torch.from_numpy(B).cuda())
+    torch.cuda.synchronize()
+    for k, st in enumerate(streams):
+        plan(ins[k], outs[k], 1.5, -0.5, st)
+    torch.cuda.synchronize()
+    for k in range(4):
+        assert_bitexact(outs[k].cpu().numpy(), wants[k], f"stream {k}")
+    A, B = make_inputs(size, perm, "s", 400)
+    want = B.copy()
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    for rep in range(150):
+        plan(dA, dB, 1.0, 0.5)
+        oracle.transpose(A, want, perm, size, 1.0, 0.5, dtype="s")
+    torch.cuda.synchronize()
+    assert_bitexact(dB.cpu().numpy(), want, "150 launches")
+    plan.close()

@@ -77,8 +77,39 @@ def knob_space(dtype: str, ttc_orders: int = 0) -> dict:
         # taking a fifth of the candidates, so the search leaves them to explicit schedules
         "tile_variant": [0],
         "loop_order": [0, 1, 2, 3],
-        "blocks": [0, 2 * SMS, 3 * SMS],
+        "blocks": [0],
+        # the staged kernel's ring depth x CTAs per SM besides the planner's: the `schedules` pairs
+        # whose tiles in motion come closest to the planner's target (see schedule_alternatives)
+        "schedules": 3,
     }
+
+
+TARGET_IN_FLIGHT = 18 * 1024 * 1024  # the planner's target for the bytes of tiles in motion
+
+
+def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
+    """Up to k (stages, ctas_per_sm) pairs other than the planner's own for a staged-kernel tile,
+    nearest the planner's in-flight target first (W = CTAs x (stages - 1) x tile bytes), skipping
+    rings that would not fit the kernel's shared memory."""
+    t = desc.get("tile") or {}
+    if desc["kernel"] != "tile" or k <= 0 or not t.get("P"):
+        return []
+    ta, tb = split_dtype(p.dtype)
+    ea, eb = ELEM_BYTES[ta], ELEM_BYTES[tb]
+    P = t["P"]
+    tile_bytes = P * (ea + eb * (2 if p.beta_nonzero else 1))
+    stage = P * ea * 1.07 + (P * eb if p.beta_nonzero else 0)
+    mine = (t.get("stages"), t.get("ctas_per_sm") or 4)
+    opts = []
+    for S in (3, 4, 5, 6):
+        if S * stage > 200 * 1024:
+            continue
+        for c in (1, 2, 3, 4):
+            if c * (S * stage + 3 * 1024) > 227 * 1024 or (S, c) == mine:
+                continue
+            W = c * SMS * (S - 1) * tile_bytes
+            opts.append((abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
+    return [{"stages": S, "ctas_per_sm": c} for _, c, S in sorted(opts)[:k]]
 
 
 def fused_groups(p: Problem):
@@ -218,6 +249,10 @@ def candidate_tunings(p: Problem, max_impl: int = 200, space: Optional[dict] = N
                     if val:
                         tu[k] = val
                 combos.append(tu)
+            # ring depth x CTAs per SM alternatives, on the first raster (the planner's, unless the
+            # caller restricted the loop orders)
+            for sch in schedule_alternatives(p, desc, space.get("schedules", 0)):
+                combos.append(dict(shape_tu, **(orders[0] if orders else {}), **sch))
         lists.append([(tu, desc) for tu in combos])
     out = []
     depth = 0

@@ -34,7 +34,7 @@ from .core import ELEM_BYTES, plan_shapes, split_dtype
 
 MAXD = 6
 DEFAULT_MODEL = Path(__file__).resolve().parent / "data" / "cost_model.npz"
-VERSION = "ttcb-mlp-v2"
+VERSION = "ttcb-mlp-v3"
 
 
 # ------------------------------------------------------------------------------------------------
@@ -72,7 +72,7 @@ def problem_features(p: Problem, desc: dict) -> list[float]:
 
 def _shape_part(p: Problem, desc: dict) -> tuple:
     """The features of a candidate that depend only on its plan (tile shape), not on the launch
-    knobs: (static values, tile count, raster jumps (A, B) for loop orders 0, 1, 2)."""
+    knobs: (static values, tile count, tile bytes)."""
     ta, tb = split_dtype(p.dtype)
     t = desc.get("tile") or {}
     row = desc.get("row") or {}
@@ -88,46 +88,59 @@ def _shape_part(p: Problem, desc: dict) -> tuple:
     mid = [min(desc["est_cost"], 200.0) / 32.0, math.log2(max(nt, 1)) / 25.0, float(t.get("fast", 0))]
     tail = [math.log2(max(P * ELEM_BYTES[ta], 1)) / 16.0,
             math.log2(max(P / max(LA, 1), 1)) / 10.0, math.log2(max(P / max(LB, 1), 1)) / 10.0]
-    # the raster: strides (bytes) between consecutive tiles along the fastest grid dimension
+    tile_bytes = P * (ELEM_BYTES[ta] + ELEM_BYTES[tb] * (2 if p.beta_nonzero else 1))
+    return head, mid, tail, nt, tile_bytes
+
+
+def _raster_jumps(p: Problem, tuning: dict, desc: dict, groups) -> list[float]:
+    """The raster the candidate runs: whether it is the planner's choice, a preset or an explicit
+    loop order, and the strides (log2 bytes, in A and in B) between consecutive tiles along its
+    fastest and its second grid dimension."""
+    from .autotune import grid_raster, preset_order
+    ta, tb = split_dtype(p.dtype)
     fu = desc["fused"]
-    ext = t.get("ext") or []
-    jumps = []
-    for lo in (0, 1, 2):
-        order = list(range(fu["rank"]))
-        if lo == 1:
-            order = list(fu["perm"])
-        elif lo == 2:
-            order = order[::-1]
-        jA = jB = 0.0
-        for dd in order:
-            e = ext[dd] if dd < len(ext) else 0
-            if e and e == fu["size"][dd]:
-                continue  # the whole dimension is inside the tile
-            step = e if e else 1
-            jA = math.log2(max(step * fu["strideA"][dd] * ELEM_BYTES[ta], 1)) / 40.0
-            jB = math.log2(max(step * fu["strideB"][dd] * ELEM_BYTES[tb], 1)) / 40.0
-            break
-        jumps.append((jA, jB))
-    return head, mid, tail, nt, jumps
+    t = desc.get("tile") or {}
+    ext = t.get("ext") or [0] * fu["rank"]
+    if tuning.get("raster") and groups is not None:
+        order = []
+        for d in tuning["raster"]:
+            fd = next((i for i, g in enumerate(groups) if d in g), None)
+            if fd is not None and fd not in order:
+                order.append(fd)
+        kind = [0.0, 0.0, 1.0]
+    else:
+        order = preset_order(desc, tuning.get("loop_order", 0))
+        kind = [1.0 if not tuning.get("loop_order") else 0.0, 1.0 if tuning.get("loop_order") else 0.0, 0.0]
+    grid = list(grid_raster(desc, order)) if desc["kernel"] == "tile" else []
+    out = []
+    for g in range(2):
+        if g < len(grid):
+            dd = grid[g]
+            step = ext[dd] if ext[dd] else 1
+            out += [math.log2(max(step * fu["strideA"][dd] * ELEM_BYTES[ta], 1)) / 40.0,
+                    math.log2(max(step * fu["strideB"][dd] * ELEM_BYTES[tb], 1)) / 40.0]
+        else:
+            out += [0.0, 0.0]
+    return kind + out
 
 
-# loop_order knob value -> raster slot of the features (0 A-major, 1 B-major, 2 reverse A)
-RASTER_SLOT = {3: 0, 1: 1, 2: 2}
-
-
-def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None) -> list[float]:
-    head, mid, tail, nt, jumps = shape or _shape_part(p, desc)
+def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None, groups=None) -> list[float]:
+    head, mid, tail, nt, tile_bytes = shape or _shape_part(p, desc)
+    t = desc.get("tile") or {}
     tv = tuning.get("tile_variant", 0)
-    # raster actually used: the knob, or the planner's choice that the shape-only plan reports
-    lo = RASTER_SLOT.get(tuning.get("loop_order", 0) or desc.get("loop_order", 3), 0)
     bl = tuning.get("blocks", 0)
+    # the staged kernel's schedule: ring depth and CTAs per SM (the knobs, else the planner's),
+    # and the bytes of tiles the whole GPU keeps in motion with them
+    S = tuning.get("stages", 0) or t.get("stages", 3) or 3
+    c = tuning.get("ctas_per_sm", 0) or t.get("ctas_per_sm", 0) or 4
+    c = min(c, 4)
+    ctas = bl if bl else c * 148
+    W = ctas * (S - 1) * tile_bytes
     f = head + [1.0 if tv == 0 else 0.0, 1.0 if tv == 2 else 0.0, 1.0 if tv == 1 else 0.0,
-                1.0 if lo == 0 else 0.0, 1.0 if lo == 1 else 0.0, 1.0 if lo == 2 else 0.0,
-                1.0 if bl == 0 else 0.0, bl / 444.0] + mid
-    # waves of the grid (CTAs: the knob, else about four resident per SM) and the last wave's fill
-    waves = nt / (bl if bl else 4 * 148)
+                1.0 if bl == 0 else 0.0, bl / 444.0, S / 6.0, c / 4.0, math.log2(max(W, 1)) / 30.0] + mid
+    waves = nt / ctas
     f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves)] + tail
-    f += list(jumps[lo])
+    f += _raster_jumps(p, tuning, desc, groups)
     return f
 
 
@@ -151,11 +164,15 @@ def features(p: Problem, cands) -> np.ndarray:
     pf = problem_features(p, cands[0][1])
     shapes = {}
     rows = []
+    groups = None
+    if any(tu.get("raster") for tu, _ in cands):
+        from .autotune import fused_groups
+        groups = fused_groups(p)[2]
     for tu, d in cands:
         sh = shapes.get(id(d))
         if sh is None:
             sh = shapes[id(d)] = _shape_part(p, d)
-        rows.append(pf + candidate_features(p, tu, d, sh))
+        rows.append(pf + candidate_features(p, tu, d, sh, groups))
     return np.asarray(rows, dtype=np.float32)
 
 
@@ -425,6 +442,49 @@ def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, v
     results = measure(p, chosen, reps=3, verify=verify) if (measure_choice or fallback) else []
     return {"results": results, "confidence": conf, "fallback": fallback, "pred": pred, "order": order,
             "candidates": cands, "seconds_model": t_model, "seconds": time.perf_counter() - t0}
+
+
+def fresh_head_to_head(cases: list[dict], model: Optional[MLP] = None, max_impl: int = 64, reps: int = 5,
+                       threshold: float = 0.1, topk: int = 2) -> dict:
+    """The selector against the method without it, on fresh timings: per problem, every candidate
+    is timed (the exhaustive search, TTC's method), then the search's winner, the network's top-1,
+    the selector's choice (top-1 when confident, else the faster of its top-(k-1) and the default,
+    timed) and the planner default are re-timed alternately, so the winner loses the bias of being the
+    maximum of noisy timings. Returns the mean shares of the winner's GB/s and the tuning times."""
+    from .autotune import search
+    model = model or load_default()
+    rows = []
+    for c in cases:
+        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
+        sr = search(p, max_impl=max_impl, reps=3, verify=False)
+        top = select(p, max_impl=max_impl, confidence=0.0, model=model, verify=False, measure_choice=False)
+        sel = select(p, max_impl=max_impl, confidence=threshold, topk=topk, model=model, verify=False,
+                     measure_choice=False)
+        top1 = top["candidates"][int(top["order"][0])][0]
+        chosen = min(sel["results"], key=lambda r: r.time_ms).tuning if sel["results"] else top1
+        picks = [sr["best"].tuning, top1, chosen, {}]
+        bench = Bench(p, seed=1)
+        best_ms = [float("inf")] * len(picks)
+        for rnd in range(2):
+            order = list(range(len(picks))) if rnd == 0 else list(reversed(range(len(picks))))
+            for i, r in zip(order, measure(p, [picks[i] for i in order], reps=reps, verify=False, bench=bench)):
+                best_ms[i] = min(best_ms[i], r.time_ms)
+        del bench
+        rows.append({"search_s": sr["seconds"], "top1_s": top["seconds"], "sel_s": sel["seconds"],
+                     "top1": best_ms[0] / best_ms[1], "sel": best_ms[0] / best_ms[2], "dflt": best_ms[0] / best_ms[3],
+                     "fallback": bool(sel["fallback"])})
+    m = lambda k: float(np.mean([r[k] for r in rows]))
+    return {"problems": len(rows), "search_candidates": max_impl,
+            "top1_over_search": round(m("top1"), 4), "selector_over_search": round(m("sel"), 4),
+            "default_over_search": round(m("dflt"), 4),
+            "selector_within_5pct": round(float(np.mean([r["sel"] >= 0.95 for r in rows])), 4),
+            "top1_within_5pct": round(float(np.mean([r["top1"] >= 0.95 for r in rows])), 4),
+            "fallbacks": int(sum(r["fallback"] for r in rows)),
+            "search_seconds_mean": round(m("search_s"), 3), "selector_seconds_mean": round(m("sel_s"), 4),
+            "top1_seconds_mean": round(m("top1_s"), 4),
+            "tuning_time_ratio_selector": round(m("search_s") / max(m("sel_s"), 1e-9), 1),
+            "tuning_time_ratio_top1": round(m("search_s") / max(m("top1_s"), 1e-9), 1),
+            "timing": f"fresh: winner, top-1, selector choice and default re-timed alternately, best of 2x{reps} launches"}
 
 
 # seeds of the training problems and of the held-out problems (ttc_b200.workloads.learning_cases)

@@ -87,7 +87,8 @@ struct RowDesc {
 };
 
 enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };
-// launch-time variant of a tile plan (never stored in a plan's kernel field)
-// Launch-time kernel choices for tile plans: register-prefetch kernel, staged kernel with offsets
-// computed from the run tables, staged kernel with offsets held in registers.
-enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5, TTCB_KERNEL_TILE_RAGGED = 6 };
+// Launch-time kernel choices for tile plans (never stored in a plan's kernel field): register-prefetch
+// kernel, staged kernel with offsets computed from the run tables or held in registers, each staged
+// form with the fixed round-robin tile order or with tiles claimed in order from a counter (_DYN).
+enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5, TTCB_KERNEL_TILE_RAGGED = 6,
+       TTCB_KERNEL_TILE_ASYNC_DYN = 7, TTCB_KERNEL_TILE_ASYNC_REG_DYN = 8 };

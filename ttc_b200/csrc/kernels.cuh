@@ -519,10 +519,18 @@ constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileIn
 // per vector from the run tables in shared memory, with the gather positions in registers while
 // P <= kRegPos * kThreads and in shared memory beyond. The number of stages (3 to kMaxStages) is the
 // descriptor's.
-template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG>
+// DYN: tiles are claimed in order from a counter in global memory (sched[0]) as the CTA goes, instead
+// of the fixed round-robin blockIdx.x + k * gridDim.x. CTAs then stay on neighbouring tiles however
+// their speeds differ, so the tiles in motion stay within a narrow span of A and B, and the last
+// tiles go to whichever CTAs are free. Each claim is issued one iteration before its result is
+// used; the last CTA to finish (sched[1] counts them) sets both words back to zero for the next
+// launch that uses them, which runs after this grid completes (stream order, and griddepcontrol.wait
+// before the first claim when the launch overlaps its predecessor).
+template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN>
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
     tile_async_kernel(
-    const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta) {
+    const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta,
+    unsigned int* __restrict__ sched) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
   __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both
@@ -675,7 +683,22 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   // (k - 2) every thread finished writing out before the barrier of iteration k - 1. Tiles are
   // decoded in batches (see TileInfo).
   const int D = S - 2;
-  if (tid < kInfoRing) decode_into(blockIdx.x + tid * G, info[tid]);
+  unsigned int pending = 0;  // DYN: thread 0's claim for the tile of iteration k + D + 3
+  if constexpr (DYN) {
+    // claims touch no tensor data, but the previous launch's reset of the counter must be visible
+    pdl_wait_previous();
+    if (tid < 32) {
+      unsigned int base = 0;
+      if (tid == 0) {
+        base = atomicAdd(&sched[0], (unsigned int)(D + 2));
+        pending = atomicAdd(&sched[0], 1u);
+      }
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (tid < D + 2) decode_into(base + tid, info[tid]);
+    }
+  } else {
+    if (tid < kInfoRing) decode_into(blockIdx.x + tid * G, info[tid]);
+  }
   __syncthreads();
   // everything above reads the plan's descriptor only; A and B are touched from here on
   pdl_wait_previous();
@@ -686,8 +709,12 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   int cur = 0;   // stage of tile k
   int nxt = D;   // stage of tile k + D
   for (uint32_t k = 0;; ++k) {
-    const uint32_t t = blockIdx.x + k * G;
-    if (t >= ntiles) break;
+    if constexpr (DYN) {
+      if (info[k % kInfoRing].state < 0) break;  // claims grow, so every later one is past the end too
+    } else {
+      const uint32_t t = blockIdx.x + k * G;
+      if (t >= ntiles) break;
+    }
     issue(info[(k + D) % kInfoRing], nxt);
     cp_async_commit();
     // tile k's copies are complete once at most D groups (tiles k + 1 .. k + D) are pending
@@ -699,8 +726,17 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       default: cp_async_wait<5>(); break;
     }
     __syncthreads();
-    if (tid < kDecodeBatch && k % kDecodeBatch == 0 && k != 0)
-      decode_into(t + (kDecodeBatch + tid) * G, info[(k + kDecodeBatch + tid) % kInfoRing]);
+    if constexpr (DYN) {
+      // the tile of iteration k + D + 2 (read after the next barrier), and the next claim
+      if (tid == 0) {
+        decode_into(pending, info[(k + D + 2) % kInfoRing]);
+        pending = atomicAdd(&sched[0], 1u);
+      }
+    } else {
+      const uint32_t t = blockIdx.x + k * G;
+      if (tid < kDecodeBatch && k % kDecodeBatch == 0 && k != 0)
+        decode_into(t + (kDecodeBatch + tid) * G, info[(k + kDecodeBatch + tid) % kInfoRing]);
+    }
     const TileInfo& ti = info[k % kInfoRing];
     TB* Bt = B + ti.bB;
     const unsigned char* stage = smem_raw + cur * sbytes;
@@ -751,6 +787,17 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     nxt = nxt + 1 == S ? 0 : nxt + 1;
   }
   cp_async_wait<0>();
+  if constexpr (DYN) {
+    // every claim of this CTA is done; the last CTA to get here resets the counter words
+    if (tid == 0) {
+      __threadfence();
+      if (atomicAdd(&sched[1], 1u) == gridDim.x - 1) {
+        atomicExch(&sched[0], 0u);
+        atomicExch(&sched[1], 0u);
+        __threadfence();
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------------

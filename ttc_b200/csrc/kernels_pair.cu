@@ -53,7 +53,7 @@ using TB = float2;
 #define PAIR_BATCH_FN pick_batch_zc
 #endif
 
-template <int VA, int VB, bool BETA, bool STREAM, bool REG>
+template <int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN>
 static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
                                 cudaStream_t stream, int blocks) {
   TA al;
@@ -61,6 +61,11 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   TB be;
   std::memset(&be, 0, sizeof(TB));
   if (BETA) std::memcpy(&be, beta, sizeof(TB));
+  unsigned int* sched = nullptr;
+  if (DYN) {
+    sched = plan_claim_slot(p);
+    if (!sched) return cudaErrorInvalidValue;
+  }
   // programmatic stream serialization: the kernel may start while the previous one in the stream
   // drains; it waits (griddepcontrol.wait) before it touches A or B
   cudaLaunchConfig_t cfg = {};
@@ -73,41 +78,41 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG>,
+  return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG, DYN>,
                             reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A),
-                            static_cast<TB*>(B), al, be);
+                            static_cast<TB*>(B), al, be, sched);
 }
 
-template <int VA, int VB, bool REG>
+template <int VA, int VB, bool REG, bool DYN>
 static KernelRef async_ref(int variant) {
   KernelRef r;
   if (variant == 2) {
-    r.fn = &launch_async<VA, VB, true, false, REG>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, REG>);
+    r.fn = &launch_async<VA, VB, true, false, REG, DYN>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, REG, DYN>);
   } else if (variant == 1) {
-    r.fn = &launch_async<VA, VB, false, true, REG>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, REG>);
+    r.fn = &launch_async<VA, VB, false, true, REG, DYN>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, REG, DYN>);
   } else {
-    r.fn = &launch_async<VA, VB, false, false, REG>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, REG>);
+    r.fn = &launch_async<VA, VB, false, false, REG, DYN>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, REG, DYN>);
   }
   return r;
 }
 
-template <int VA, bool REG>
+template <int VA, bool REG, bool DYN>
 static KernelRef async_ref_b(int vb, int variant) {
   constexpr int MB = 16 / sizeof(TB);
-  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), REG>(variant);
-  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), REG>(variant);
-  return async_ref<VA, 1, REG>(variant);
+  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), REG, DYN>(variant);
+  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), REG, DYN>(variant);
+  return async_ref<VA, 1, REG, DYN>(variant);
 }
 
-template <bool REG>
+template <bool REG, bool DYN>
 static KernelRef async_ref_ab(int va, int vb, int variant) {
   constexpr int MA = 16 / sizeof(TA);
-  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), REG>(vb, variant);
-  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), REG>(vb, variant);
-  return async_ref_b<1, REG>(vb, variant);
+  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), REG, DYN>(vb, variant);
+  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), REG, DYN>(vb, variant);
+  return async_ref_b<1, REG, DYN>(vb, variant);
 }
 
 template <int VA, int VB, bool BETA, bool STREAM, bool FAST>
@@ -231,8 +236,10 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
     return row_ref<1>(variant);
   }
   if (kernel == TTCB_KERNEL_TILE_FAST) return tile_ref_ab<true>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false, false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true, false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_DYN) return async_ref_ab<false, true>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG_DYN) return async_ref_ab<true, true>(va, vb, variant);
   if (kernel == TTCB_KERNEL_TILE_RAGGED) return ragged_ref(variant);
   return tile_ref_ab<false>(va, vb, variant);
 }

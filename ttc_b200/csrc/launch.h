@@ -19,6 +19,13 @@ struct KernelRef {
 // One definition per A/B type pair lives in kernels_<pair>.cu.
 KernelRef pick_kernel(ttcb_dtype ta, ttcb_dtype tb, int kernel, int va, int vb, int variant);
 
+// The counter words (claim, finished CTAs) of the next launch of a plan's staged kernel with claimed
+// tiles: one of the plan's kClaimSlots slot pairs, taken in turn, so launches of one plan on
+// different streams use different words (up to kClaimSlots of them in flight). Null when the plan
+// has no counters.
+constexpr int kClaimSlots = 64;
+unsigned int* plan_claim_slot(const ttcb_plan* p);
+
 // Dynamic shared memory ceiling of every plan (the planner never exceeds it).
 constexpr int kMaxDynamicSmem = 200 * 1024;
 // True when a launch with this much dynamic shared memory needs the opt-in above 48 KB.

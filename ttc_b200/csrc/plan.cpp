@@ -445,6 +445,61 @@ void plan_tile_cache_end() {
 }
 
 // ------------------------------------------------------------------------------------------------
+// Planning constants of the staged kernel's schedule: the B200's SM count and the bytes of tiles
+// the whole GPU keeps in motion (see build_tile_desc).
+static constexpr int kPlanSMs = 148;
+static constexpr double kTargetInFlightBytes = 18.0 * 1024 * 1024;
+
+// Ring depth S and CTAs per SM c of the staged kernel. Every resident CTA keeps S - 1 tiles in its
+// ring (S - 2 of copies in flight and the one being written), so the tiles in motion on the whole
+// GPU span W = c * SMs * (S - 1) * tile bytes of A and B. Timed over the 64-case 200 MiB sweep
+// (every S in 3..6 x c in 1..4), the fastest schedules keep W near 18 MiB: less leaves HBM without
+// enough requests, more spreads the concurrent accesses over more DRAM pages and costs 5-15%.
+// Tiles whose accesses are 16 bytes wide on both sides reach W with few CTAs; narrower accesses need
+// every CTA an SM holds for instruction issue, so only S is chosen for them. Problems too small to
+// fill the GPU twice keep the most CTAs and the earlier rule (four stages while four CTAs fit, else
+// three). smem_for(S) is the dynamic shared memory of an S-stage ring; fixed_S (3..kMaxStages, else
+// 0) is a schedule's explicit ring depth. c = 0 means as many CTAs as fit.
+struct StageChoice {
+  int S = 3;
+  int c = 0;
+};
+
+template <typename SmemFn>
+static StageChoice choose_stages(int64_t P, int EA, int EB, bool beta, int vecA, int vecB, int64_t nfull,
+                                 const SmemFn& smem_for, int fixed_S) {
+  StageChoice out;
+  out.S = smem_for(4) <= 56 * 1024 ? 4 : 3;
+  const bool fixed = fixed_S >= 3 && fixed_S <= ttcb::kMaxStages;
+  const int64_t tile_bytes = P * (int64_t)(EA + EB * (beta ? 2 : 1));
+  const bool wide = vecA * EA == 16 && vecB * EB == 16;
+  const int reg_ctas = ttcb::async_min_blocks(vecA * EA, vecB * EB, beta);
+  double best = 1e30;
+  int bS = 0, bc = 0;
+  for (int S = 3; S <= 6; ++S) {
+    if (fixed && S != fixed_S) continue;
+    if (smem_for(S) > 200 * 1024) continue;
+    const int64_t per_cta = smem_for(S) + (int64_t)ttcb::kAsyncStaticSmem + 1024;
+    const int cmax = (int)std::min<int64_t>(reg_ctas, (227 * 1024) / per_cta);
+    if (cmax < 1) continue;
+    for (int cc = wide ? 1 : cmax; cc <= cmax; ++cc) {
+      const double W = (double)cc * kPlanSMs * (S - 1) * (double)tile_bytes;
+      const double key = std::fabs(std::log(W / kTargetInFlightBytes));
+      if (key < best - 1e-9) {
+        best = key;
+        bS = S;
+        bc = cc;
+      }
+    }
+  }
+  if (bS && nfull >= 2LL * 4 * kPlanSMs) {
+    out.S = bS;
+    out.c = bc;
+  }
+  if (fixed) out.S = fixed_S;
+  return out;
+}
+
 static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   const FusedProblem& f = p->f;
   std::vector<int> aord, bord;
@@ -692,10 +747,12 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     auto smem_for = [&](int S) {
       return (int64_t)ttcb::async_smem_bytes(S, td.stage_elems, (int)P, (int)nsegA, (int)nsegB, EA, EB, beta);
     };
-    // four stages (two tiles of copies in flight) while four CTAs still fit an SM (about 56 KB
-    // each), else three (one tile in flight); deeper rings (up to ttcb::kMaxStages) measured
-    // slower on the sweep, with four CTAs or with fewer
-    td.nstages = smem_for(4) <= 56 * 1024 ? 4 : 3;
+    {
+      const StageChoice sc = choose_stages(P, EA, dtype_bytes(p->tb), beta, c.vecA, c.vecB, td.nfull, smem_for,
+                                           p->tuning.stages);
+      td.nstages = sc.S;
+      p->ctas_per_sm = p->tuning.ctas_per_sm > 0 ? p->tuning.ctas_per_sm : sc.c;
+    }
     if (p->tuning.stages >= 3 && p->tuning.stages <= ttcb::kMaxStages) td.nstages = p->tuning.stages;
     td.async_ok = (mA < (int64_t(1) << 31) && mB < (int64_t(1) << 31) && td.stage_elems < 65536 &&
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
@@ -944,6 +1001,24 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
     p->vecA = best.vecA;
     p->vecB = best.vecB;
     p->est_cost = best.cost;
+    // the staged kernel's ring depth and CTAs per SM, from the staged layout's usual size (the bank
+    // padding adds about 6% to a tile; the exact size needs the full descriptor)
+    int64_t nfull = 1;
+    for (int d = 0; d < f.rank; ++d) {
+      if (best.ext[d] == 0)
+        nfull *= f.n[d];
+      else if (best.ext[d] < f.n[d])
+        nfull *= f.n[d] / best.ext[d];
+    }
+    const int64_t P = best.P, stage_elems = P + P / 16;
+    const int EBb = dtype_bytes(p->tb);
+    auto smem_for = [&](int S) {
+      return (int64_t)ttcb::async_smem_bytes(S, (int)stage_elems, (int)P, (int)(P / best.LA), (int)(P / best.LB), EA,
+                                             EBb, beta);
+    };
+    const StageChoice sc = choose_stages(P, EA, EBb, beta, best.vecA, best.vecB, nfull, smem_for, p->tuning.stages);
+    p->shape_stages = sc.S;
+    p->ctas_per_sm = p->tuning.ctas_per_sm > 0 ? p->tuning.ctas_per_sm : sc.c;
     return TTCB_OK;
   }
   build_tile_desc(p, best, EA);
@@ -1029,13 +1104,14 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
       << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
-      << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
+      << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
   } else if (p->kernel == TTCB_KERNEL_TILE && p->shape_only) {
     const bool fits = p->tile_P / p->vecA <= 1024 && p->tile_P / p->vecB <= 1024;
     o << ",\"tile\":{\"P\":" << p->tile_P << ",\"LA\":" << p->tile_LA << ",\"LB\":" << p->tile_LB
-      << ",\"ntiles\":" << p->tile_ntiles << ",\"fast\":" << (fits ? 1 : 0) << ",\"shape_only\":1,\"ext\":[";
+      << ",\"ntiles\":" << p->tile_ntiles << ",\"fast\":" << (fits ? 1 : 0) << ",\"stages\":" << p->shape_stages
+      << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"shape_only\":1,\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {

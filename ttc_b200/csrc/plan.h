@@ -64,6 +64,7 @@ struct ttcb_plan {
   int blocks_fast = 0;    // CTAs for the fast tile kernel
   int smem_async = 0;     // staged tile kernel (stages + tables)
   int blocks_async = 0;   // CTAs for the staged tile kernel
+  int ctas_per_sm = 0;    // staged tile kernel: CTAs per SM the schedule asks for (0 = as many as fit)
   int blocks_ragged = 0;  // CTAs for the ragged-tile kernel that runs beside the staged kernel
   // the ragged-tile kernel runs on a side stream forked from (and joined back into) the caller's
   // stream; the mutex keeps one call's record/wait sequence whole when calls come from several threads
@@ -71,6 +72,10 @@ struct ttcb_plan {
   void* ev_fork = nullptr;      // cudaEvent_t
   void* ev_join = nullptr;      // cudaEvent_t
   void* fork_mutex = nullptr;   // std::mutex
+  // staged kernel with claimed tiles: kClaimSlots pairs of counter words on the device (zeroed at
+  // creation, reset by each launch's last CTA) and the host's running launch count
+  unsigned int* claim_words = nullptr;
+  void* launch_count = nullptr;  // std::atomic<unsigned int>
   int smem_ragged = 0;    // its dynamic shared memory (two tile buffers + tables)
   int device = 0;
 
@@ -89,6 +94,7 @@ struct ttcb_plan {
   bool shape_only = false;
   int64_t tile_P = 0, tile_LA = 0, tile_LB = 0, tile_ntiles = 0;
   int64_t tile_ext[TTCB_MAXR] = {0};  // tile extent per fused dimension (0 = not in the tile)
+  int shape_stages = 0;                // the staged kernel's ring depth the schedule would use
 };
 
 // Fills everything except dev_desc / blocks (which need the CUDA device). Returns a status and a
