@@ -2,7 +2,7 @@
 
 Recipe (runs where the TTC sources are: `python -m oracle.make_ref [TTC_SOURCE_DIR] [--count N]`,
 the directory defaulting to $TTC_REFERENCE_DIR, else the reference checkout of this machine):
-  1. convert the TTC package to Python 3 in a scratch directory (oracle/ttc_py3.py);
+  1. convert the TTC package to Python 3 in a scratch directory (ttc_b200/py2compat.py);
   2. for each case of the 64-case sweep (the workload bench.py times), run TTC's own driver
      `ttc.main()` with `--architecture=avx --compiler=g++` and its default `--maxImplementations=200`:
      TTC generates its AVX variants, compiles them with its Makefile (g++ -O3 -fopenmp -march=native),
@@ -32,7 +32,7 @@ ROOT = HERE.parent
 REF_DIR = HERE / "_ref"
 sys.path.insert(0, str(ROOT))
 
-from oracle import ttc_py3  # noqa: E402
+from ttc_b200 import py2compat as ttc_py3  # noqa: E402
 
 # Where this recipe reads the TTC sources unless told otherwise.
 DEFAULT_SOURCE = os.environ.get("TTC_REFERENCE_DIR", "/root/reference")

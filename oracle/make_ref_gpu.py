@@ -2,7 +2,7 @@
 
 Recipe (runs where the TTC sources are: `python -m oracle.make_ref_gpu [TTC_SOURCE_DIR]`):
   1. import TTC's CUDA generator (GPUtransposeGenerator.py, CUDAtranspose.py, converted to Python 3
-     by oracle/ttc_py3.py);
+     by ttc_b200/py2compat.py);
   2. for each case of the 64-case sweep, fuse its indices with TTC's fuseIndices (ttc_util.py:214-276)
      and let the generator enumerate its variants the way `ttc --architecture=cuda` does
      (GPUtransposeGenerator.py:165-230, 328-349: TTC's blockings sorted by its blocking cost, every
@@ -35,7 +35,7 @@ ROOT = HERE.parent
 REF_DIR = HERE / "_ref"
 sys.path.insert(0, str(ROOT))
 
-from oracle import ttc_py3  # noqa: E402
+from ttc_b200 import py2compat as ttc_py3  # noqa: E402
 from oracle.make_ref import DEFAULT_SOURCE, MAX_IMPL, case_key, sweep_cases  # noqa: E402
 
 VARIANTS_PER_CASE = 8

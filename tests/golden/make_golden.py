@@ -2,7 +2,7 @@
 
 TTC's correctness oracle is a C++ loop nest that its GPU generator emits for every transposition
 (GPUreference.referenceTranspose, GPUreference.py:33-244 in the TTC project). This script imports
-that generator from the TTC sources (converted to Python 3 by oracle/ttc_py3.py), emits the loop for each
+that generator from the TTC sources (converted to Python 3 by ttc_b200/py2compat.py), emits the loop for each
 case of TTC's own test matrix (test-framework/ttc_test.py:80-92, first size of every permutation,
 every dtype pair and beta of the sweep) plus padded lda/ldb cases, compiles all of them into one
 host program with g++ (cuComplex.h from the CUDA toolkit for the complex types, no -march, so no
@@ -27,7 +27,7 @@ sys.path.insert(0, str(HERE.parent))
 sys.path.insert(0, str(HERE.parent.parent))
 
 import helpers  # noqa: E402
-from oracle import ttc_py3  # noqa: E402
+from ttc_b200 import py2compat as ttc_py3  # noqa: E402
 
 OUT = HERE / "ttc_reference_loop.npz"
 CU_TYPES = {"s": "float", "d": "double", "c": "cuFloatComplex", "z": "cuDoubleComplex"}

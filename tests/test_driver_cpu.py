@@ -129,3 +129,45 @@ def test_loop_perm_flags_become_explicit_rasters():
     assert all("raster" in t for t in cands)
     b = ttc.parse_args(["--perm=1,0,2", "--size=1000,768,16"])
     assert ttc._tunings_from_args(b, "s")["rasters"] == ("ttc", 2)
+
+
+def test_report_summarises_the_fastest_variants_per_rank(tmp_path, capsys):
+    """TTC's benchmark summary (generatePlots.py:141-265) over the fastest0Percent view: per rank the
+    bandwidth range of the fastest variants and their speedup over the reference bandwidth."""
+    from ttc_b200 import report
+    db = str(tmp_path / "ttc.db")
+    v = lambda bw: [{"tuning": {}, "bandwidth": bw, "time": 1e-3, "rank": 0},
+                    {"tuning": {"run_bytes": 128}, "bandwidth": bw / 2, "time": 2e-3, "rank": 1}]
+    sql_util.insert(db, [100, 200, 30], [1, 0, 2], "float", "float", 1.0, 0.0, "dev", "h", v(100.0), 1.0, 50.0)
+    sql_util.insert(db, [10, 20, 30], [2, 1, 0], "float", "float", 1.0, 0.0, "dev", "h", v(300.0), 1.0, 100.0)
+    sql_util.insert(db, [64, 64], [1, 0], "double", "double", 1.0, 0.0, "dev", "h", v(40.0), 1.0)
+    rows = report.benchmark_summary(db)
+    assert [r["dim"] for r in rows] == [2, 3]
+    r3 = rows[1]
+    assert (r3["count"], r3["bw_min"], r3["bw_max"], r3["bw_avg"]) == (2, 100.0, 300.0, 200.0)
+    assert (r3["speedup_min"], r3["speedup_max"]) == (2.0, 3.0)
+    assert rows[0]["speedup_count"] == 0  # no reference bandwidth recorded
+    out = tmp_path / "s.csv"
+    assert report.main(["--db", db, "--csv", str(out)]) == 0
+    assert "avg GiB/s" in capsys.readouterr().out and out.read_text().startswith("dim,count")
+    assert report.benchmark_summary(db, "floatTypeA = 'double'")[0]["count"] == 1
+
+
+def test_cpu_architecture_runs_ttcs_own_generator(tmp_path, monkeypatch, capsys):
+    """--architecture=avx goes, with the same flags, to TTC's own CPU driver (ttc.py:1132-1376) from a
+    TTC checkout: it generates, compiles, checks and times its variants and writes the header; without
+    a checkout the request fails with a message instead of silently running on the GPU."""
+    from oracle.make_ref import DEFAULT_SOURCE
+    from pathlib import Path
+    argv = ["--perm=1,0,2", "--size=64,48,5", "--architecture=avx", "--compiler=g++", "--maxImplementations=2",
+            "--numThreads=2", "--ignoreDatabase"]
+    monkeypatch.chdir(tmp_path)
+    monkeypatch.setenv("TTC_SOURCE_DIR", str(tmp_path / "nowhere"))
+    assert ttc.main(argv) == 1
+    assert "TTC_SOURCE_DIR" in capsys.readouterr().out
+    if not (Path(DEFAULT_SOURCE) / "ttc" / "ttc.py").exists():
+        pytest.skip("the TTC sources are not on this machine")
+    monkeypatch.setenv("TTC_SOURCE_DIR", DEFAULT_SOURCE)
+    name, gibps = ttc.generateTransposition(ttc.parse_args(argv))
+    assert gibps > 0 and (tmp_path / "ttc_transpositions" / f"{name}.h").exists()
+    assert "implementations done" in capsys.readouterr().out

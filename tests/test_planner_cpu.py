@@ -353,7 +353,7 @@ def test_search_adds_ttc_ranked_loop_orders():
     cands = candidate_tunings(p, 500, knob_space("s", ttc_orders=2), with_desc=True)
     by_shape = {}
     for tu, d in cands:
-        if d["kernel"] != "tile" or "stages" in tu:  # ring/CTA alternatives reuse the first raster
+        if d["kernel"] != "tile" or "stages" in tu or "round_robin" in tu:  # schedule alternatives reuse the first raster
             continue
         key = json.dumps({k: v for k, v in tu.items() if k in ("tile_elems", "run_bytes")}, sort_keys=True)
         by_shape.setdefault(key, (d, []))[1].append(tu)

@@ -99,17 +99,20 @@ def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
     P = t["P"]
     tile_bytes = P * (ea + eb * (2 if p.beta_nonzero else 1))
     stage = P * ea * 1.07 + (P * eb if p.beta_nonzero else 0)
-    mine = (t.get("stages"), t.get("ctas_per_sm") or 4)
+    cmax = lambda S: max(1, min(4, int(227 * 1024 // (S * stage + 3 * 1024))))
+    mine = (t.get("stages"), t.get("ctas_per_sm") or cmax(t.get("stages") or 3))
     opts = []
     for S in (3, 4, 5, 6):
         if S * stage > 200 * 1024:
             continue
-        for c in (1, 2, 3, 4):
-            if c * (S * stage + 3 * 1024) > 227 * 1024 or (S, c) == mine:
+        for c in (2, 3, 4):
+            if c > cmax(S) or (S, c) == mine:
                 continue
             W = c * SMS * (S - 1) * tile_bytes
-            opts.append((abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
-    return [{"stages": S, "ctas_per_sm": c} for _, c, S in sorted(opts)[:k]]
+            # fewer CTAs than fit cost the sweep 2-12%, so they come after every full-occupancy ring
+            opts.append((c != cmax(S), abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
+    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]]
+    return out + [{"round_robin": 1}]
 
 
 def fused_groups(p: Problem):

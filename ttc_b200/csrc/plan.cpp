@@ -452,14 +452,14 @@ static constexpr double kTargetInFlightBytes = 18.0 * 1024 * 1024;
 
 // Ring depth S and CTAs per SM c of the staged kernel. Every resident CTA keeps S - 1 tiles in its
 // ring (S - 2 of copies in flight and the one being written), so the tiles in motion on the whole
-// GPU span W = c * SMs * (S - 1) * tile bytes of A and B. Timed over the 64-case 200 MiB sweep
-// (every S in 3..6 x c in 1..4), the fastest schedules keep W near 18 MiB: less leaves HBM without
-// enough requests, more spreads the concurrent accesses over more DRAM pages and costs 5-15%.
-// Tiles whose accesses are 16 bytes wide on both sides reach W with few CTAs; narrower accesses need
-// every CTA an SM holds for instruction issue, so only S is chosen for them. Problems too small to
-// fill the GPU twice keep the most CTAs and the earlier rule (four stages while four CTAs fit, else
-// three). smem_for(S) is the dynamic shared memory of an S-stage ring; fixed_S (3..kMaxStages, else
-// 0) is a schedule's explicit ring depth. c = 0 means as many CTAs as fit.
+// GPU span W = c * SMs * (S - 1) * tile bytes of A and B. The planner keeps every CTA an SM holds
+// (c = 0: timed over the whole 64-case 200 MiB sweep back to back, fewer CTAs per SM lost 2% with
+// three and 12% with two, although single cases repeated alone ran faster with them) and picks the
+// S in 3..6 whose W comes nearest 18 MiB: with S fixed at 3 or 4 for every case the sweep measured
+// within 0.5% of this rule, and for single cases rings far from it lost 5-15%. Problems too small to
+// fill the GPU twice keep the earlier rule (four stages while four CTAs fit, else three).
+// smem_for(S) is the dynamic shared memory of an S-stage ring; fixed_S (3..kMaxStages, else 0) is a
+// schedule's explicit ring depth.
 struct StageChoice {
   int S = 3;
   int c = 0;
@@ -472,30 +472,23 @@ static StageChoice choose_stages(int64_t P, int EA, int EB, bool beta, int vecA,
   out.S = smem_for(4) <= 56 * 1024 ? 4 : 3;
   const bool fixed = fixed_S >= 3 && fixed_S <= ttcb::kMaxStages;
   const int64_t tile_bytes = P * (int64_t)(EA + EB * (beta ? 2 : 1));
-  const bool wide = vecA * EA == 16 && vecB * EB == 16;
   const int reg_ctas = ttcb::async_min_blocks(vecA * EA, vecB * EB, beta);
   double best = 1e30;
-  int bS = 0, bc = 0;
+  int bS = 0;
   for (int S = 3; S <= 6; ++S) {
     if (fixed && S != fixed_S) continue;
     if (smem_for(S) > 200 * 1024) continue;
     const int64_t per_cta = smem_for(S) + (int64_t)ttcb::kAsyncStaticSmem + 1024;
     const int cmax = (int)std::min<int64_t>(reg_ctas, (227 * 1024) / per_cta);
     if (cmax < 1) continue;
-    for (int cc = wide ? 1 : cmax; cc <= cmax; ++cc) {
-      const double W = (double)cc * kPlanSMs * (S - 1) * (double)tile_bytes;
-      const double key = std::fabs(std::log(W / kTargetInFlightBytes));
-      if (key < best - 1e-9) {
-        best = key;
-        bS = S;
-        bc = cc;
-      }
+    const double W = (double)cmax * kPlanSMs * (S - 1) * (double)tile_bytes;
+    const double key = std::fabs(std::log(W / kTargetInFlightBytes));
+    if (key < best - 1e-9) {
+      best = key;
+      bS = S;
     }
   }
-  if (bS && nfull >= 2LL * 4 * kPlanSMs) {
-    out.S = bS;
-    out.c = bc;
-  }
+  if (bS && nfull >= 2LL * 4 * kPlanSMs) out.S = bS;
   if (fixed) out.S = fixed_S;
   return out;
 }

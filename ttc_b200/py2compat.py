@@ -1,10 +1,12 @@
-"""TEST INFRASTRUCTURE - loads modules of the TTC sources (Python 2) under Python 3.
+"""Runs modules of the TTC sources (Python 2) under Python 3.
 
-Copies the requested files from the TTC project into a scratch directory, expands tabs (the sources
+Copies the requested files from a TTC checkout into a scratch directory, expands tabs (the sources
 mix tabs and spaces), and rewrites the Python 2 constructs they use: print statements, integer `/`,
 `dict.has_key`, list-returning `range`, implicit relative imports, byte-string subprocess output.
-Used by tests/golden/make_golden.py and oracle/make_ref.py where the TTC sources exist; nothing at
-test or bench time reads the TTC sources.
+The command line uses it to hand `--architecture=avx|avx512|knc|power` requests to TTC's own CPU
+code generator (ttc_b200.cpu_delegate); the build recipes of the CPU and GPU reference arms and the
+golden fixtures (oracle/make_ref.py, oracle/make_ref_gpu.py, tests/golden/make_golden.py) use it to
+drive TTC's generators. Nothing on the GPU path reads the TTC sources.
 """
 from __future__ import annotations
 

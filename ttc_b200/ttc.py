@@ -209,10 +209,16 @@ def generateTransposition(ttcArgs: TTCargs):
     from .core import plan_host_json
 
     a = ttcArgs
+    if a.architecture != "cuda" and getattr(a, "architectureGiven", False):
+        # a CPU architecture asked for explicitly: TTC's own CPU generator does the work
+        from . import cpu_delegate
+        if a.compiler == "nvcc":
+            a.compiler = "g++"
+        return cpu_delegate.generate(a, echo=not a.silent)
     if a.architecture != "cuda":
         if not a.silent:
-            print(WARNING + "[TTC] WARNING: this implementation targets the GPU -> switching architecture to cuda."
-                  + ENDC)
+            print(WARNING + "[TTC] WARNING: this implementation targets the GPU -> switching architecture to cuda "
+                  "(--architecture=avx runs TTC's own CPU generator)." + ENDC)
         a.architecture = "cuda"
     a.compiler = "nvcc"
     if a.maxNumImplementations == -1:
@@ -356,6 +362,7 @@ def parse_args(argv) -> TTCargs:
             if val not in ("avx", "knc", "avx512", "power", "cuda"):
                 raise TTCError(1, "[TTC] ERROR: Architecture unknown.")
             o["arch"] = val
+            o["arch_given"] = True
         elif key == "--compiler":
             if val not in ("icpc", "g++", "ibm", "nvcc"):
                 raise TTCError(1, "[TTC] ERROR: unknown compiler choice.")
@@ -410,6 +417,7 @@ def parse_args(argv) -> TTCargs:
     a.maxNumImplementations = o["maxImpl"]
     a.floatTypeA, a.floatTypeB = o["floatA"], o["floatB"]
     a.architecture, a.compiler = o["arch"], o["compiler"]
+    a.architectureGiven = bool(o.get("arch_given"))
     a.lda, a.ldb = o["lda"], o["ldb"]
     a.blockings, a.loopPermutations, a.vecLength = o["blockings"], o["loopPerms"], o["vec"]
     a.numThreads, a.affinity, a.prefetchDistances = o["numThreads"], o["affinity"], o["prefetch"]
