@@ -86,7 +86,10 @@ typedef struct {
                             0 = planner's choice. `blocks`, when set, takes precedence          */
   int32_t round_robin;   /* staged tile kernel: 0 = CTAs claim tiles in order from a counter the
                             plan owns, 1 = fixed round-robin order (tile blockIdx + k * CTAs)    */
-  int32_t reserved[2];
+  int32_t shifted_runs;  /* staged tile kernel: 0 = planner's choice (A runs that 16-byte
+                            accesses cannot reach directly are copied as the 16-byte chunks that
+                            cover them), -1 = never                                            */
+  int32_t reserved[1];
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

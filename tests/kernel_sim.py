@@ -20,10 +20,10 @@ _layout = None
 def layout():
     global _layout
     if _layout is None:
-        a = (ctypes.c_int64 * 12)()
+        a = (ctypes.c_int64 * 13)()
         _native.lib().ttcb_test_desc_layout(a)
         keys = ["tile_size", "off_divLA", "off_g", "g_size", "off_bd", "bd_size", "row_size", "row_off_div",
-                "row_off_sA", "row_off_sB", "fastdiv_size", "g_strideA"]
+                "row_off_sA", "row_off_sB", "fastdiv_size", "g_strideA", "off_shiftA"]
         _layout = dict(zip(keys, list(a)))
     return _layout
 
@@ -106,7 +106,35 @@ def parse_tile(b):
     t["segB"] = np.frombuffer(b, dtype=np.int64, count=t["nsegB"], offset=t["off_segB"])
     t["ptab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_perm"]).astype(np.int64)
     t["gtab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_gtab"]).astype(np.int64)
+    o = L["off_shiftA"]
+    t["shiftA"], t["shiftW"], t["shiftCM"] = _i32(b, o), _i32(b, o + 4), _i32(b, o + 8)
     return t
+
+
+def check_shifted_layout(t, p_of_q, V):
+    """Shifted A runs: for every tile shift x in 0..V-1, replay the load phase (chunk c of run s is
+    copied when lo <= x < hi, from A element segA[s] - y + V*c - x past the tile base into slot
+    s*W + V*c, y = segA[s] mod V) and check that the gather at gtab[q] + x finds A element
+    segA[s] + j of position p(q) = s*LA + j, that every copied chunk overlaps its run (so no copy
+    leaves the 16-byte blocks the run touches) and that nothing lies beyond the stage."""
+    P, LA, W, CM = t["P"], t["LA"], t["shiftW"], t["shiftCM"]
+    nseg = P // LA
+    segA = t["segA"].astype(np.int64)
+    y = segA % V
+    assert W % V == 0 and W >= CM * V and nseg * W <= t["stage_elems"]
+    for x in range(V):
+        src = np.full(t["stage_elems"] + V, -(1 << 60), np.int64)
+        for s in range(nseg):
+            for c in range(CM):
+                lo, hi = c * V - y[s] - LA + 1, (c + 1) * V - y[s]
+                if not (lo <= x < hi):
+                    continue
+                first = segA[s] - y[s] + V * c - x  # A element (from the tile base) of the chunk's first slot
+                assert first + V > segA[s] and first < segA[s] + LA, "a copied chunk misses its run"
+                src[s * W + V * c: s * W + V * c + V] = first + np.arange(V)
+        s_of, j_of = p_of_q // LA, p_of_q % LA
+        got = src[t["gtab"] + x]
+        assert np.array_equal(got, segA[s_of] + j_of), f"shift {x}: a gather reads an element it was not given"
 
 
 def check_staged_layout(t, vecA):
@@ -119,6 +147,9 @@ def check_staged_layout(t, vecA):
     inv[t["ptab"]] = np.arange(P, dtype=np.int64)
     p_of_q = inv[slot_q]
     assert (p_of_q >= 0).all()
+    if t["shiftA"]:
+        check_shifted_layout(t, p_of_q, vecA)
+        return
     stg = p_of_q + (p_of_q // t["sigmaA"]) * t["padA"]
     assert np.array_equal(stg, t["gtab"]), "gtab disagrees with the staged layout"
     assert len(np.unique(t["gtab"])) == P and t["gtab"].max() < t["stage_elems"]

@@ -41,7 +41,7 @@ def test_largest_default_descriptors_fit_the_scratch_array():
     """Descriptor bytes = header + 8 per A and B run segment + 4 per tile element; the planner caps a
     default tile at 16 KiB of A elements and 1024 segments a side, so no default plan comes near
     64 KiB. Checked on the tiles the planner picks for a few extreme shapes."""
-    layout = (ctypes.c_int64 * 12)()
+    layout = (ctypes.c_int64 * 13)()
     _native.lib().ttcb_test_desc_layout(layout)
     header = layout[0]
     worst = 0

@@ -340,8 +340,8 @@ def test_claimed_tiles_with_concurrent_launches_and_slot_reuse():
     import torch
     from ttc_b200 import Plan
     perm, size = [2, 0, 1], [67, 45, 311]
-    plan = Plan(perm, size, "s", True, tuning={"ctas_per_sm": 1})
-    assert plan.describe()["tile"]["async"] == 1
+    plan = Plan(perm, size, "s", True, tuning={"blocks": 16})  # many tiles per CTA: claims on
+    assert plan.describe()["tile"]["async"] == 1 and plan.describe()["tile"]["claims"] == 1
     n = int(np.prod(size))
     streams = [torch.cuda.Stream() for _ in range(4)]
     ins, outs, wants = [], [], []
@@ -365,3 +365,23 @@ def test_claimed_tiles_with_concurrent_launches_and_slot_reuse():
     torch.cuda.synchronize()
     assert_bitexact(dB.cpu().numpy(), want, "150 launches")
     plan.close()
+
+
+SHIFTED = [([1, 0], [99, 1001]), ([1, 0, 3, 2], [99, 17, 35, 3]), ([1, 0, 2], [45, 77, 9]),
+           ([2, 1, 0], [10, 25, 2097]), ([0, 2, 1], [31, 110, 15]), ([2, 0, 1], [23, 13, 240])]
+
+
+@pytest.mark.parametrize("dtype", ["s", "d", "c", "sd", "ds", "cz"])
+def test_shifted_a_runs(dtype):
+    """A runs of odd lengths and offsets copied as the 16-byte chunks that cover them, shifted per
+    tile (and by A's own misalignment, offsets of 1 to 3 elements): bit for bit against the oracle,
+    for beta = 0 and beta != 0, and equal to the plain layout (shifted_runs = -1)."""
+    used = 0
+    for perm, size in SHIFTED:
+        for beta in (0.0, -0.5):
+            for offset in (0, 1, 3):
+                desc = check_case(perm, size, dtype, 1.5, beta, offset=offset)
+                used += int((desc.get("tile") or {}).get("shifted_runs", 0))
+            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": -1})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 0, "round_robin": 1, "stages": 5})
+    assert used > 0

@@ -62,7 +62,8 @@ class Tuning(ctypes.Structure):
                 ("vec", ctypes.c_int32), ("blocks", ctypes.c_int32), ("loop_order", ctypes.c_int32),
                 ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("ragged", ctypes.c_int32),
                 ("raster_lo", ctypes.c_int32), ("raster_hi", ctypes.c_int32), ("stages", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("round_robin", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
+                ("ctas_per_sm", ctypes.c_int32), ("round_robin", ctypes.c_int32),
+                ("shifted_runs", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":

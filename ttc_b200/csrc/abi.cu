@@ -89,6 +89,7 @@ using ttcb::needs_large_smem;
 // The staged kernel claims tiles from the plan's counters unless the schedule asks for the fixed
 // round-robin order or the plan has none.
 static bool uses_claims(const ttcb_plan* p) { return p->claim_words && p->tuning.round_robin != 1; }
+static constexpr int kClaimMinTilesPerCta = 16;
 
 static ttcb_status plan_finish_device(ttcb_plan* p) {
   if (p->empty) return TTCB_OK;
@@ -151,7 +152,14 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (s != TTCB_OK) return s;
     }
     if (td->async_ok) {
-      if (p->tuning.round_robin != 1) {
+      // Tiles are claimed in order only when every CTA has many of them (a problem of 200 MiB has
+      // 20 to 150 per CTA): the claims helped the 200 MiB sweep by about 1%, but a CTA claims its
+      // first S tiles at once, which on problems of a few tiles per CTA leaves most CTAs idle (1 to
+      // 4 MiB problems lost a quarter of their speed).
+      s = grid_for(td->reg_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async,
+                   &p->blocks_async, td->nfull);
+      if (s != TTCB_OK) return s;
+      if (p->tuning.round_robin != 1 && td->nfull >= (int64_t)kClaimMinTilesPerCta * p->blocks_async) {
         e = cudaMalloc(&p->claim_words, sizeof(unsigned int) * 2 * ttcb::kClaimSlots);
         if (e != cudaSuccess) {
           p->claim_words = nullptr;
@@ -201,7 +209,10 @@ static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const
   const int EA = dtype_bytes(p->ta), EB = dtype_bytes(p->tb);
   cudaError_t e;
   int va = p->vecA, vb = p->vecB;
-  while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
+  const bool shifted = p->kernel == TTCB_KERNEL_TILE &&
+                       reinterpret_cast<const TileDesc*>(p->host_desc.data())->shiftA;
+  // shifted A runs take any pointer (the kernel folds its misalignment into the tile shift)
+  while (!shifted && va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
   while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
   if (p->kernel == TTCB_KERNEL_ROW) va = vb = std::min(va, vb);
   int kernel = p->kernel, blocks = p->blocks, smem = p->smem_bytes;
@@ -209,6 +220,8 @@ static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const
     const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
     const int want = p->tuning.tile_variant;
     const bool fast_ok = td->fast && td->P / va <= 1024 && td->P / vb <= 1024;
+    if (shifted && !((want == 0 || want == 3) && td->async_ok))
+      return fail(TTCB_ERR_UNSUPPORTED, "a plan with shifted A runs runs only on the staged tile kernel");
     if ((want == 0 || want == 3) && td->async_ok) {
       const bool claims = uses_claims(p);
       kernel = (fast_ok && td->reg_ok) ? (claims ? TTCB_KERNEL_TILE_ASYNC_REG_DYN : TTCB_KERNEL_TILE_ASYNC_REG)
@@ -608,6 +621,7 @@ void ttcb_test_desc_layout(int64_t* out) {
   out[9] = offsetof(RowDesc, sB);
   out[10] = sizeof(FastDiv);
   out[11] = offsetof(GridDimDesc, strideA);
+  out[12] = offsetof(TileDesc, shiftA);
 }
 
 uint32_t ttcb_test_fastdiv(uint32_t n, uint32_t d) {

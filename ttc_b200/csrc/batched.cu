@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/ttcb200.h"
@@ -118,6 +119,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
     void* B;
     int full_only;  // the plan's complete tiles only (its edge plans follow it)
     int user;       // index of the caller's plan
+    int own;        // 1: the caller's plan itself (0: one of its edge plans)
   };
   std::vector<Entry> ent;
   ent.reserve(count);
@@ -140,12 +142,56 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
       return bfail(TTCB_ERR_INVALID_ARG, "A or B of problem " + std::to_string(i) + " is NULL");
     }
     const bool edges = !p->empty && p->kernel == TTCB_KERNEL_TILE && p->nedge > 0;
-    ent.push_back({p, A[i], B[i], edges ? 1 : 0, i});
+    ent.push_back({p, A[i], B[i], edges ? 1 : 0, i, 1});
     for (int k = 0; edges && k < p->nedge; ++k) {
       const ttcb_plan* q = p->edge[k];
       ent.push_back({q, static_cast<const char*>(A[i]) + q->base_offA * EA,
-                     static_cast<char*>(B[i]) + q->base_offB * EB, 0, i});
+                     static_cast<char*>(B[i]) + q->base_offB * EB, 0, i, 0});
     }
+  }
+  // The batched kernel stages A in the plain layout (element p at p + (p / sigmaA) * padA); a plan
+  // with shifted A runs takes part through a host copy of itself planned without them.
+  std::vector<std::unique_ptr<ttcb_plan>> unshifted;
+  for (Entry& e : ent) {
+    const ttcb_plan* p = e.p;
+    if (p->empty || p->kernel != TTCB_KERNEL_TILE) continue;
+    if (!reinterpret_cast<const TileDesc*>(p->host_desc.data())->shiftA) continue;
+    std::unique_ptr<ttcb_plan> q(new (std::nothrow) ttcb_plan());
+    if (!q) {
+      batch_free(b);
+      return bfail(TTCB_ERR_ALLOC, "host allocation of a batch problem failed");
+    }
+    q->rank = p->rank;
+    for (int i = 0; i < p->rank; ++i) {
+      q->perm[i] = p->perm[i];
+      q->size[i] = p->size[i];
+      q->lda[i] = p->lda[i];
+      q->ldb[i] = p->ldb[i];
+    }
+    q->ta = p->ta;
+    q->tb = p->tb;
+    q->beta_nonzero = p->beta_nonzero;
+    q->tuning = p->tuning;
+    q->tuning.shifted_runs = -1;
+    q->depth = p->depth;
+    q->base_offA = p->base_offA;
+    q->base_offB = p->base_offB;
+    q->device = p->device;
+    std::string err;
+    if (plan_build_host(q.get(), err) != TTCB_OK || q->kernel != TTCB_KERNEL_TILE ||
+        q->host_desc.size() < sizeof(TileDesc)) {
+      batch_free(b);
+      return bfail(TTCB_ERR_UNSUPPORTED, "a batch problem could not be planned for the batched kernel: " + err);
+    }
+    // the batch moves the complete tiles of the same grid: the tile must not change
+    const TileDesc* a = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    const TileDesc* c = reinterpret_cast<const TileDesc*>(q->host_desc.data());
+    if (a->P != c->P || a->ntiles != c->ntiles || a->nfull != c->nfull) {
+      batch_free(b);
+      return bfail(TTCB_ERR_UNSUPPORTED, "a batch problem planned without shifted runs changed its tiles");
+    }
+    e.p = q.get();
+    unshifted.push_back(std::move(q));
   }
   const int n = (int)ent.size();
   b->count = n;
@@ -190,7 +236,7 @@ ttcb_status ttcb_batch_create(ttcb_batch** out, int count, const ttcb_plan* cons
             max_slots_bytes, (int)ttcb::al16((size_t)std::max(td->stage_elems, td->phys_size) * EA));
         max_table_bytes = std::max<int>(max_table_bytes, 8 * (td->nsegA + td->nsegB) + 4 * ((td->P + 1) / 2));
       }
-      if (p == plans[ent[i].user]) b->bytes += ttcb_plan_bytes(p);  // an edge plan's bytes are its parent's
+      if (ent[i].own) b->bytes += ttcb_plan_bytes(p);  // an edge plan's bytes are its parent's
     }
     prefix[i + 1] = prefix[i] + items;
   }

@@ -71,6 +71,17 @@ struct TileDesc {
   FastDiv divSigmaA;
   GridDimDesc g[TTCB_MAXR];
   BlockedDesc bd[2];
+  // staged kernel, shifted A runs (A runs that 16-byte accesses cannot reach directly: odd lengths or
+  // offsets): each run is copied as the 16-byte chunks that cover it. Run s keeps chunk slots
+  // [s * shiftW, s * shiftW + shiftCM * V) (V = 16 / sizeof(TA)); a tile whose first A element lies
+  // x elements past a 16-byte boundary (x = (a0 + tile base) mod V, a0 the misalignment of A's
+  // pointer) puts element j of run s at s * shiftW + (segA[s] mod V) + x + j, which is gtab's position
+  // plus x: the store phase reads through the stage base moved by x elements.
+  int32_t shiftA;     // 1: A runs are copied as covering 16-byte chunks (the vector width is V)
+  int32_t shiftW;     // staged stride of one A run (elements, a multiple of V)
+  int32_t shiftCM;    // chunk slots per A run
+  int32_t shift_pad_;
+  FastDiv divCM;      // divisor shiftCM
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
 };
 

@@ -526,11 +526,12 @@ constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileIn
 // used; the last CTA to finish (sched[1] counts them) sets both words back to zero for the next
 // launch that uses them, which runs after this grid completes (stream order, and griddepcontrol.wait
 // before the first claim when the launch overlaps its predecessor).
+// a0 (shifted A runs only): A's pointer is a0 elements past a 16-byte boundary.
 template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN>
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
     tile_async_kernel(
     const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta,
-    unsigned int* __restrict__ sched) {
+    unsigned int* __restrict__ sched, int a0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
   __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both
@@ -562,13 +563,18 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       }
     }
   }
-  const int nvA = P / VA, nvB = P / VB;
+  const bool shift = VA * sizeof(TA) == 16 && d.shiftA;
+  // A copies per tile: VA-element vectors, or with shifted runs the chunk slots of every run
+  const int nvA = shift ? d.nsegA * d.shiftCM : P / VA, nvB = P / VB;
   constexpr int kVecB = REG ? kRegVec : kRegPos / VB;  // B vectors per thread with positions in gp
   constexpr int kGp = (kVecB * VB + 1) / 2;
   // gather positions: byte offsets in the register path, element positions otherwise
   uint32_t gp[kGp];
   int32_t rA[REG ? kRegVec : 1], rB[REG ? kRegVec : 1];
   uint32_t dA[REG ? kRegVec / 2 : 1];
+  // the tile shifts x for which each of the thread's A copies is made: x in [lo, hi), 4-bit fields
+  // (lo + 1, hi) per copy; without shifted runs a copy is made at x = 0 when it exists
+  uint32_t lohi = 0;
 #pragma unroll
   for (int e = 0; e < kGp; ++e) gp[e] = 0;
   if (reg_pos) {
@@ -595,12 +601,23 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       const int i = tid + u * kThreads;
       rA[u] = rB[u] = 0;
       if (!(u & 1)) dA[u >> 1] = 0;
-      if (i < nvA) {
+      if (i < nvA && shift) {
+        // chunk c of run s: source V * (segA[s] / V + c) past the tile's aligned base, slot
+        // s * shiftW + V * c; it covers run elements for lo <= x < hi
+        const int s = (int)fdiv((uint32_t)i, d.divCM);
+        const int c = i - s * d.shiftCM;
+        const int y = (int)(gA[s] & (VA - 1));
+        rA[u] = (int32_t)(gA[s] - y) + VA * c;
+        dA[u >> 1] |= ((uint32_t)(s * d.shiftW + VA * c) * (uint32_t)sizeof(TA)) << ((u & 1) * 16);
+        const int lo = max(c * VA - y - LA + 1, -1), hi = min((c + 1) * VA - y, VA + 1);
+        lohi |= ((uint32_t)(lo + 1) | ((uint32_t)max(hi, 0) << 4)) << (8 * u);
+      } else if (i < nvA) {
         const int p = i * VA;
         const int s = (int)fdiv((uint32_t)p, divLA);
         const int sp = (int)fdiv((uint32_t)p, divSig);
         rA[u] = (int32_t)(gA[s] + (p - s * LA));
         dA[u >> 1] |= ((uint32_t)(p + sp * padA) * (uint32_t)sizeof(TA)) << ((u & 1) * 16);
+        lohi |= (1u | (1u << 4)) << (8 * u);  // x = 0 is in [0, 1)
       }
       if (i < nvB) {
         const int q = i * VB;
@@ -623,9 +640,13 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     ti.state = 1;
   };
 
+  // the tile's shift: its first A element lies x elements past a 16-byte boundary (shifted runs)
+  auto shift_of = [&](const TileInfo& ti) -> int { return shift ? (int)((a0 + ti.bA) & (VA - 1)) : 0; };
+
   auto issue = [&](const TileInfo& ti, int stage) {
     if (ti.state != 1) return;  // ragged tiles are moved by the ragged-tile kernel
-    const TA* At = A + ti.bA;
+    const int x = shift_of(ti);
+    const TA* At = A + (ti.bA - x);  // 16-byte aligned with shifted runs
     const TB* Bt = B + ti.bB;
     const uint32_t sb = stage0 + (uint32_t)stage * sbytes;
     const uint32_t sbB = sb + a_bytes;
@@ -633,17 +654,30 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
 #pragma unroll
       for (int u = 0; u < kRegVec; ++u) {
         const int i = tid + u * kThreads;
-        if (i < nvA) cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu), At + rA[u]);
+        const uint32_t f = lohi >> (8 * u);
+        if (x + 1 >= (int)(f & 15u) && x < (int)((f >> 4) & 15u))
+          cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu), At + rA[u]);
         if (BETA && i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
       }
     } else {
       const int LA = d.LA, LB = d.LB, padA = d.padA;
       const FastDiv divLA = d.divLA, divLB = d.divLB, divSig = d.divSigmaA;
-      for (int i = tid; i < nvA; i += kThreads) {
-        const int p = i * VA;
-        const int s = (int)fdiv((uint32_t)p, divLA);
-        const int sp = (int)fdiv((uint32_t)p, divSig);
-        cp_async<VA * sizeof(TA)>(sb + (uint32_t)((p + sp * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+      if (shift) {
+        for (int i = tid; i < nvA; i += kThreads) {
+          const int s = (int)fdiv((uint32_t)i, d.divCM);
+          const int c = i - s * d.shiftCM;
+          const int y = (int)(segA[s] & (VA - 1));
+          if (x >= c * VA - y - LA + 1 && x < (c + 1) * VA - y)
+            cp_async<VA * sizeof(TA)>(sb + (uint32_t)((s * d.shiftW + VA * c) * sizeof(TA)),
+                                      At + (segA[s] - y + VA * c));
+        }
+      } else {
+        for (int i = tid; i < nvA; i += kThreads) {
+          const int p = i * VA;
+          const int s = (int)fdiv((uint32_t)p, divLA);
+          const int sp = (int)fdiv((uint32_t)p, divSig);
+          cp_async<VA * sizeof(TA)>(sb + (uint32_t)((p + sp * padA) * sizeof(TA)), At + (segA[s] + (p - s * LA)));
+        }
       }
       if (BETA) {
         for (int i = tid; i < nvB; i += kThreads) {
@@ -733,8 +767,10 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     }
     const TileInfo& ti = info[k % kInfoRing];
     TB* Bt = B + ti.bB;
-    const unsigned char* stage = smem_raw + cur * sbytes;
-    const TB* sB = reinterpret_cast<const TB*>(stage + a_bytes);
+    const unsigned char* stage_base = smem_raw + cur * sbytes;
+    const TB* sB = reinterpret_cast<const TB*>(stage_base + a_bytes);
+    // gathers read the A data through the stage base moved by the tile's shift
+    const unsigned char* stage = stage_base + shift_of(ti) * (int)sizeof(TA);
     if (ti.state == 1) {
       if constexpr (REG) {
 #pragma unroll

@@ -78,9 +78,11 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  // shifted A runs: A's pointer lies a0 elements past a 16-byte boundary
+  const int a0 = (int)(((uintptr_t)A / sizeof(TA)) & (uintptr_t)(VA - 1));
   return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG, DYN>,
                             reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A),
-                            static_cast<TB*>(B), al, be, sched);
+                            static_cast<TB*>(B), al, be, sched, a0);
 }
 
 template <int VA, int VB, bool REG, bool DYN>

@@ -124,7 +124,7 @@ extern "C" ttcb_status ttcb_transpose_noalloc(int rank, const int* perm, const i
   p.device = dev;
 
   int va = p.vecA, vb = p.vecB;
-  while (va > 1 && (uintptr_t)A % (va * EA)) va /= 2;
+  while (!td->shiftA && va > 1 && (uintptr_t)A % (va * EA)) va /= 2;  // shifted runs take any pointer
   while (vb > 1 && (uintptr_t)B % (vb * EB)) vb /= 2;
   const bool reg = td->reg_ok && td->P / va <= 1024 && td->P / vb <= 1024;
   const int kernel = reg ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC;

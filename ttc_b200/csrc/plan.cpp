@@ -493,6 +493,14 @@ static StageChoice choose_stages(int64_t P, int EA, int EB, bool beta, int vecA,
   return out;
 }
 
+// Shifted A runs (TileDesc::shiftA) for a tile whose A runs 16-byte accesses cannot reach directly
+// but that are at least two 16-byte chunks long, on the staged kernel only.
+static bool wants_shifted_runs(const TileCand& c, int EA, const ttcb_tuning& tu) {
+  const int VM = 16 / EA;
+  return EA < 16 && c.vecA < VM && c.LA >= 2 * VM && tu.vec != 1 && tu.shifted_runs != -1 &&
+         (tu.tile_variant == 0 || tu.tile_variant == 3);
+}
+
 static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   const FusedProblem& f = p->f;
   std::vector<int> aord, bord;
@@ -550,6 +558,18 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   const int EAw = EA >= 4 ? EA / 4 : 1;
   int64_t sigma = c.LA;
   auto staged = [&](int64_t pp, int64_t padA) { return pp + (pp / sigma) * padA; };
+  // Shifted A runs: when 16-byte accesses cannot reach A's runs directly (their length or offsets
+  // are not multiples of V = 16 / EA elements) but the runs are at least 2V long, each run is copied
+  // as the 16-byte chunks that cover it (see TileDesc::shiftA): up to LA / V + 2 copies instead of LA
+  // (fp32) or LA / 2 (fp64) narrow ones. Run s then sits at s * shiftW + (segA[s] mod V).
+  const int VM = 16 / EA;
+  const bool shift = wants_shifted_runs(c, EA, p->tuning);
+  const int64_t CM = shift ? (2 * VM - 3 + c.LA) / VM + 1 : 0;  // chunk slots per run
+  int64_t shiftW = CM * VM;
+  auto staged_shift = [&](int64_t pp, int64_t W) {
+    const int64_t s = pp / c.LA;
+    return s * W + (((segA[s] % VM) + VM) % VM) + (pp - s * c.LA);
+  };
   // A warp's 8-byte loads are served per half-warp and its 16-byte loads per quarter-warp, so the
   // wavefronts of one load are the sum over those lane groups of the busiest bank's count.
   const int group = 32 / EAw;
@@ -564,7 +584,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
           for (int lane = g0; lane < g0 + group; ++lane) {
             int64_t i = (int64_t)w * 32 + lane;
             if (i * vb >= P) continue;
-            int64_t word = staged(p_of_q[i * vb + j], padA) * EAw;
+            int64_t word = (shift ? staged_shift(p_of_q[i * vb + j], shiftW + padA)
+                                  : staged(p_of_q[i * vb + j], padA)) * EAw;
             for (int x = 0; x < EAw; ++x) {
               int b = (int)((word + x) & 31);
               mx = std::max(mx, ++cnt[b]);
@@ -592,8 +613,22 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
         for (int g0 = 0; g0 < 32; g0 += group)
           if (((int64_t)w * 32 + g0) * c.vecB < P) ++ideal;
     int64_t best_cost = -1, best_sigma = c.LA, best_pad = 0;
+    if (shift) {
+      // the run stride: the chunk slots plus 0..8 chunks of padding, the fewest conflicts
+      for (int k = 0; k <= 8; ++k) {
+        const int64_t cand = (int64_t)k * VM;
+        if ((P / c.LA) * (shiftW + cand) > 65535) break;
+        const int64_t cc = gather_cost(cand);
+        if (best_cost < 0 || cc < best_cost) {
+          best_cost = cc;
+          best_pad = cand;
+        }
+        if (best_cost == ideal) break;
+      }
+      shiftW += best_pad;
+    }
     for (int64_t sg : sigmas) {
-      if (best_cost == ideal) break;
+      if (shift || best_cost == ideal) break;
       sigma = sg;
       for (int k = 0; k <= 8; ++k) {
         const int64_t cand = (int64_t)k * c.vecA;
@@ -608,12 +643,13 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
         if (best_cost == ideal) break;
       }
     }
-    sigma = best_sigma;
-    padA = best_pad;
+    sigma = shift ? c.LA : best_sigma;
+    padA = shift ? 0 : best_pad;
   }
-  const int64_t staged_size = staged(P - 1, padA) + 1;
+  const int64_t staged_size = shift ? (P / c.LA) * shiftW : staged(P - 1, padA) + 1;
   std::vector<uint16_t> gtab(P);
-  for (int64_t q = 0; q < P; ++q) gtab[q] = (uint16_t)staged(p_of_q[q], padA);
+  for (int64_t q = 0; q < P; ++q)
+    gtab[q] = (uint16_t)(shift ? staged_shift(p_of_q[q], shiftW) : staged(p_of_q[q], padA));
   for (int64_t s = 0; s < nsegB; ++s) {
     int64_t rem = s * c.LB, offB = 0;
     for (int d : bord) {
@@ -626,6 +662,10 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
 
   TileDesc td;
   std::memset(&td, 0, sizeof(td));
+  td.shiftA = shift ? 1 : 0;
+  td.shiftW = (int32_t)(shift ? shiftW : 0);
+  td.shiftCM = (int32_t)CM;
+  td.divCM = make_fastdiv((uint32_t)std::max<int64_t>(CM, 1));
   td.P = (int32_t)P;
   td.LA = (int32_t)c.LA;
   td.LB = (int32_t)c.LB;
@@ -741,7 +781,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       return (int64_t)ttcb::async_smem_bytes(S, td.stage_elems, (int)P, (int)nsegA, (int)nsegB, EA, EB, beta);
     };
     {
-      const StageChoice sc = choose_stages(P, EA, dtype_bytes(p->tb), beta, c.vecA, c.vecB, td.nfull, smem_for,
+      const StageChoice sc = choose_stages(P, EA, dtype_bytes(p->tb), beta, shift ? VM : c.vecA, c.vecB, td.nfull, smem_for,
                                            p->tuning.stages);
       td.nstages = sc.S;
       p->ctas_per_sm = p->tuning.ctas_per_sm > 0 ? p->tuning.ctas_per_sm : sc.c;
@@ -751,6 +791,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
     td.reg_ok = (td.fast && td.stage_elems * (int64_t)EA < 65536 && P * (int64_t)EB < 65536) ? 1 : 0;
+    // with shifted runs every chunk slot is a copy: the register path holds four per thread
+    if (shift && (P / c.LA) * CM > 4 * 256) td.reg_ok = 0;
     // the staged kernel leaves ragged tiles to the ragged-tile kernel, whose tables must fit too
     if (td.nrag0 + td.nrag1 > 0 && ttcb::ragged_smem_bytes((int)phys_size, EA, (int)P) > 200 * 1024) td.async_ok = 0;
   }
@@ -764,7 +806,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   p->smem_bytes = (int)smem;
   p->smem_fast = (int)al16(phys_size * EA);
   p->smem_ragged = (int)ttcb::ragged_smem_bytes((int)phys_size, EA, (int)P);
-  p->vecA = c.vecA;
+  p->vecA = shift ? VM : c.vecA;  // shifted runs copy 16-byte chunks
   p->vecB = c.vecB;
   p->est_cost = c.cost;
 }
@@ -991,7 +1033,8 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   p->tile_ntiles = ntiles;
   for (int d = 0; d < f.rank; ++d) p->tile_ext[d] = best.ext[d];
   if (p->shape_only) {
-    p->vecA = best.vecA;
+    p->vecA = wants_shifted_runs(best, EA, p->tuning) ? 16 / EA : best.vecA;
+    p->shape_shifted = wants_shifted_runs(best, EA, p->tuning);
     p->vecB = best.vecB;
     p->est_cost = best.cost;
     // the staged kernel's ring depth and CTAs per SM, from the staged layout's usual size (the bank
@@ -1009,12 +1052,22 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
       return (int64_t)ttcb::async_smem_bytes(S, (int)stage_elems, (int)P, (int)(P / best.LA), (int)(P / best.LB), EA,
                                              EBb, beta);
     };
-    const StageChoice sc = choose_stages(P, EA, EBb, beta, best.vecA, best.vecB, nfull, smem_for, p->tuning.stages);
+    const StageChoice sc = choose_stages(P, EA, EBb, beta, p->vecA, best.vecB, nfull, smem_for, p->tuning.stages);
     p->shape_stages = sc.S;
     p->ctas_per_sm = p->tuning.ctas_per_sm > 0 ? p->tuning.ctas_per_sm : sc.c;
     return TTCB_OK;
   }
   build_tile_desc(p, best, EA);
+  {
+    // shifted A runs exist only for the staged kernel: when it cannot run this tile (or the schedule
+    // names another tile kernel), the plan is made with the plain layout instead
+    const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
+    const int tv = p->tuning.tile_variant;
+    if (td->shiftA && (!td->async_ok || (tv != 0 && tv != 3))) {
+      p->tuning.shifted_runs = -1;
+      build_tile_desc(p, best, EA);
+    }
+  }
   return TTCB_OK;
 }
 
@@ -1097,14 +1150,17 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"pshift\":" << t->pshift << ",\"fast\":" << t->fast << ",\"async\":" << t->async_ok
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
       << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
-      << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
+      << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm
+      << ",\"shifted_runs\":" << t->shiftA << ",\"claims\":" << (p->claim_words ? 1 : 0)
+      << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
   } else if (p->kernel == TTCB_KERNEL_TILE && p->shape_only) {
     const bool fits = p->tile_P / p->vecA <= 1024 && p->tile_P / p->vecB <= 1024;
     o << ",\"tile\":{\"P\":" << p->tile_P << ",\"LA\":" << p->tile_LA << ",\"LB\":" << p->tile_LB
       << ",\"ntiles\":" << p->tile_ntiles << ",\"fast\":" << (fits ? 1 : 0) << ",\"stages\":" << p->shape_stages
-      << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"shape_only\":1,\"ext\":[";
+      << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"shifted_runs\":" << (p->shape_shifted ? 1 : 0)
+      << ",\"shape_only\":1,\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
   } else if (p->kernel == TTCB_KERNEL_ROW && !p->host_desc.empty()) {

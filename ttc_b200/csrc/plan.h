@@ -95,6 +95,7 @@ struct ttcb_plan {
   int64_t tile_P = 0, tile_LA = 0, tile_LB = 0, tile_ntiles = 0;
   int64_t tile_ext[TTCB_MAXR] = {0};  // tile extent per fused dimension (0 = not in the tile)
   int shape_stages = 0;                // the staged kernel's ring depth the schedule would use
+  bool shape_shifted = false;          // the staged kernel would copy shifted A runs
 };
 
 // Fills everything except dev_desc / blocks (which need the CUDA device). Returns a status and a

@@ -15,6 +15,7 @@ uint32_t ttcb_test_fastdiv(uint32_t n, uint32_t d);
 size_t ttcb_test_plan_host_desc(int rank, const int* perm, const int64_t* size, const int64_t* lda,
                                 const int64_t* ldb, int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning,
                                 int* kernel, void* buf, size_t len);
+// Sizes and offsets of the descriptor structs (13 entries), so host-side checkers can parse them.
 void ttcb_test_desc_layout(int64_t* out);
 // Shape-only plans of one problem under n tunings (the learned selector's candidate features):
 // writes a JSON array (one plan description per tuning, null where planning failed) into buf and
