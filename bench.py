@@ -59,17 +59,20 @@ def parse(argv=None):
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (README, strided, batched, selector) in the sweep line")
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case", "configs"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batched", "case", "configs", "batchcase"],
                     help="sweep: the 64-case 200 MiB sweep (default); batched: 4096 small transpositions "
                          "in one persistent launch against per-call launches; case: one sweep case run "
                          "--reps times with its default plan (a small command for profilers); configs: the "
-                         "README shape and the strided mixed-precision shapes, each timed alone")
+                         "README shape and the strided mixed-precision shapes, each timed alone; batchcase: the "
+                         "batched workload with the planner's schedules launched --reps times (for profilers)")
     ap.add_argument("--schedule", default="learned", choices=["default", "learned"],
                     help="sweep: the planner's default schedule per case, or the learned selector's choice "
                          "(chosen before the timed region: its top-1, timed against the planner default when "
                          "its confidence is low)")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
-    ap.add_argument("--reps", type=int, default=3, help="case: launches")
+    ap.add_argument("--reps", type=int, default=3, help="case / batchcase: launches")
+    ap.add_argument("--tuning", default=None, help="case: a schedule (JSON of ttcb_tuning fields) instead of the "
+                                                   "planner's default")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-tuning", default="search", choices=["search", "default"],
                     help="per-problem schedules: measured search (the autotuner) or the planner default")
@@ -625,8 +628,8 @@ def run_sweep(args, rank, world, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded uniform[-1,1])",
                 "pct_of_hbm_peak": round(100 * value / world / peak, 2),
                 "config": sweep_config(len(cases), bytes_per_step, world),
-                "schedules": schedule_note or ("learned selector (top-1; timed against the planner default when "
-                                               "its confidence < 0.1)" if args.schedule == "learned"
+                "schedules": schedule_note or ("learned selector (top-1 on a large predicted gain over the planner "
+                                               "default, timed against it on a moderate one)" if args.schedule == "learned"
                                                else "planner default"),
                 "schedule_seconds": round(t_sel, 1),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
@@ -640,13 +643,14 @@ def run_sweep(args, rank, world, local):
 
 # ------------------------------------------------------------------------------------------------
 def flushed_timing(plan, A, B, alpha, beta, steps, warmup, flush):
-    """Median and best ms of `steps` launches, each after writing 2x the L2 (CUDA events)."""
+    """Median and best ms of `steps` launches, each after an L2 flush (autotune.L2Flush: 2x the L2
+    written, then 2x read; CUDA events)."""
     import torch
     for _ in range(warmup):
         plan(A, B, alpha, beta)
     ms = []
     for _ in range(steps):
-        flush.zero_()
+        flush()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         plan(A, B, alpha, beta)
@@ -660,7 +664,7 @@ def configs_summary(args, steps=None, warmup=None):
     """The single-problem configurations: TTC's README shape (perm 1,0,2 / 1000,768,16, fp32,
     alpha = beta = 1) and the strided mixed-precision shape (perm 3,1,0,2 / 96,80,72,64, lda + 8,0,4,0;
     z->c with alpha = (0.5, 0.25) and d->s with alpha = 0.5, beta = 0). Inputs uniform[-1,1] from the
-    seed (B from seed + 1), resident; the L2 is flushed (2x its size written) before every timed
+    seed (B from seed + 1), resident; the L2 is flushed (2x its size written, then 2x read) before every timed
     launch; CUDA events. Returns {name: result}."""
     import torch
     import ttc_b200.workloads as wl
@@ -668,7 +672,8 @@ def configs_summary(args, steps=None, warmup=None):
     steps = steps or max(args.steps, 10)
     warmup = warmup or max(args.warmup, 3)
     tmap = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}
-    flush = torch.empty(2 * 126 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    from ttc_b200.autotune import L2Flush
+    flush = L2Flush()
     peak, _ = measured_peak_gbs()
     out = {}
     for name, c in [("readme_1000x768x16_s_beta1", wl.readme_case())] + \
@@ -690,8 +695,26 @@ def configs_summary(args, steps=None, warmup=None):
                      "alpha": str(c["alpha"]), "beta": c["beta"], "bytes": plan.bytes,
                      "GBps_median": round(gbs, 1), "GBps_best": round(plan.bytes / (best / 1e3) / 1e9, 1),
                      "frac_of_hbm_peak": round(gbs / peak, 4), "kernel": kernel_name(d), "tile": d.get("tile"),
-                     "vec": [d["vecA"], d["vecB"]], "l2": "flushed before every launch", "steps": steps}
+                     "vec": [d["vecA"], d["vecB"]], "l2": "flushed before every launch (2x L2 written, then 2x read)",
+                     "steps": steps,
+                     "schedule": "planner default"}
         plan.close()
+        # the learned selector's schedule for the same problem (as the sweep uses it)
+        try:
+            from ttc_b200 import cost_model
+            from ttc_b200.autotune import Problem
+            tu = cost_model.choose_tuning(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"],
+                                                  c.get("lda")))
+        except Exception as ex:
+            tu, out[name]["learned"] = None, {"unavailable": f"{type(ex).__name__}: {ex}"}
+        if tu:
+            lp = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, lda=c.get("lda"), tuning=tu)
+            lmed, lbest = flushed_timing(lp, A, B, c["alpha"], c["beta"], steps, warmup, flush)
+            lg = lp.bytes / (lmed / 1e3) / 1e9
+            out[name]["learned"] = {"tuning": tu, "GBps_median": round(lg, 1), "frac_of_hbm_peak": round(lg / peak, 4)}
+            lp.close()
+        elif "learned" not in out[name]:
+            out[name]["learned"] = {"tuning": {}, "note": "the selector kept the planner default"}
     return out
 
 
@@ -821,7 +844,7 @@ def run_case(args):
     gen.manual_seed(c["seed"])
     A = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen)
     B = torch.rand(n, dtype=tmap[c["dtype"]], device="cuda", generator=gen)
-    plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0)
+    plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=json.loads(args.tuning) if args.tuning else None)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.reps):
@@ -833,6 +856,30 @@ def run_case(args):
                       "beta": c["beta"], "GBps": round(plan.bytes / (ms / 1e3) / 1e9, 1), "bytes": plan.bytes,
                       "plan": plan.describe()}), flush=True)
     plan.close()
+    return 0
+
+
+def run_batchcase(args):
+    """The batched workload with the planner's schedules (no per-problem search), one persistent
+    launch `--reps` times; prints the mean GB/s (CUDA events). Meant to sit under a profiler."""
+    import torch
+    from ttc_b200.batched import Batch
+    args.batch_tuning = "default"
+    plans, As, Bs, Cs, _, cases = build_batch_problems(args, 0, torch.device("cuda"))
+    batch = Batch(plans, As, Bs, alpha=1.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.reps):
+        batch.launch()
+    e1.record()
+    torch.cuda.synchronize()
+    batch.check_status()
+    ms = e0.elapsed_time(e1) / max(args.reps, 1)
+    print(json.dumps({"workload": "batchcase", "problems": len(cases), "bytes": batch.bytes,
+                      "GBps": round(batch.bytes / (ms / 1e3) / 1e9, 1)}), flush=True)
+    batch.close()
+    for p in plans:
+        p.close()
     return 0
 
 
@@ -1004,6 +1051,8 @@ def main():
         return run_case(args)
     if args.workload == "configs":
         return run_configs(args)
+    if args.workload == "batchcase":
+        return run_batchcase(args)
     return run_sweep(args, rank, world, local)
 
 

@@ -86,9 +86,9 @@ typedef struct {
                             0 = planner's choice. `blocks`, when set, takes precedence          */
   int32_t round_robin;   /* staged tile kernel: 0 = CTAs claim tiles in order from a counter the
                             plan owns, 1 = fixed round-robin order (tile blockIdx + k * CTAs)    */
-  int32_t shifted_runs;  /* staged tile kernel: 0 = planner's choice (A runs that 16-byte
-                            accesses cannot reach directly are copied as the 16-byte chunks that
-                            cover them), -1 = never                                            */
+  int32_t shifted_runs;  /* staged tile kernel: 1 = copy A runs that 16-byte accesses cannot
+                            reach directly (odd lengths or offsets) as the 16-byte chunks that
+                            cover them; 0 = planner's choice (plain copies), -1 = never         */
   int32_t reserved[1];
 } ttcb_tuning;
 

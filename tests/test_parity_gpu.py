@@ -380,8 +380,9 @@ def test_shifted_a_runs(dtype):
     for perm, size in SHIFTED:
         for beta in (0.0, -0.5):
             for offset in (0, 1, 3):
-                desc = check_case(perm, size, dtype, 1.5, beta, offset=offset)
+                desc = check_case(perm, size, dtype, 1.5, beta, offset=offset, tuning={"shifted_runs": 1})
                 used += int((desc.get("tile") or {}).get("shifted_runs", 0))
             check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": -1})
-            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 0, "round_robin": 1, "stages": 5})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 1, "round_robin": 1, "stages": 5})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 1, "blocks": 9})  # claimed tiles
     assert used > 0

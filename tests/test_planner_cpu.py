@@ -84,7 +84,7 @@ def _oracle_pairs(perm, size, lda, ldb):
 
 
 TUNINGS = [None, {"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"tile_elems": 256}, {"tile_elems": 8192},
-           {"run_bytes": 128}, {"run_bytes": 1024}, {"kernel": 1}]
+           {"run_bytes": 128}, {"run_bytes": 1024}, {"kernel": 1}, {"shifted_runs": 1}]
 
 
 def test_kernel_index_math_replay_matches_oracle_mapping():
@@ -353,7 +353,7 @@ def test_search_adds_ttc_ranked_loop_orders():
     cands = candidate_tunings(p, 500, knob_space("s", ttc_orders=2), with_desc=True)
     by_shape = {}
     for tu, d in cands:
-        if d["kernel"] != "tile" or "stages" in tu or "round_robin" in tu:  # schedule alternatives reuse the first raster
+        if d["kernel"] != "tile" or {"stages", "round_robin", "shifted_runs"} & set(tu):  # schedule alternatives reuse the first raster
             continue
         key = json.dumps({k: v for k, v in tu.items() if k in ("tile_elems", "run_bytes")}, sort_keys=True)
         by_shape.setdefault(key, (d, []))[1].append(tu)
@@ -371,3 +371,32 @@ def test_search_adds_ttc_ranked_loop_orders():
             else:
                 rasters.append(grid_raster(d, preset_order(d, tu.get("loop_order", 0))))
         assert len(set(rasters)) == len(set(json.dumps(tu, sort_keys=True) for tu in tus if not tu.get("blocks")))
+
+
+def test_shifted_a_runs_replay():
+    """Shifted A runs (tuning shifted_runs = 1): for random problems whose A runs 16-byte accesses
+    cannot reach directly, the CPU replay of the load phase, for every tile shift, must put into each
+    gathered slot exactly the A element the store phase expects (kernel_sim.check_shifted_layout),
+    and the element mapping must equal the oracle's."""
+    rng = np.random.default_rng(11)
+    shifted = 0
+    for it in range(90):
+        perm, size, lda, ldb = _random_problem(rng, max_rank=4, max_ext=24)
+        for dtype in ("s", "d", "c"):
+            tu = {"shifted_runs": 1}
+            try:
+                kind, b = kernel_sim.host_desc(perm, size, dtype, False, lda, ldb, tu)
+            except TTCError:
+                continue
+            if kind != 1:
+                continue
+            t = kernel_sim.parse_tile(b)
+            if not t["shiftA"]:
+                continue
+            shifted += 1
+            j = plan_host_json(perm, size, dtype, False, lda, ldb, tu)
+            kernel_sim.check_staged_layout(t, j["vecA"])
+            _, (a, b) = kernel_sim.simulate(perm, size, dtype, False, lda, ldb, tu)
+            wa, wb = _oracle_pairs(perm, size, lda, ldb)
+            assert dict(zip(b.tolist(), a.tolist())) == dict(zip(wb.tolist(), wa.tolist()))
+    assert shifted >= 30

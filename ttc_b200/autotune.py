@@ -24,6 +24,25 @@ SMS = 148
 L2_BYTES = 126 * 1024 * 1024
 
 
+class L2Flush:
+    """Evicts the L2 between timed launches: writes a buffer twice the L2's size, then reads another
+    one as large. The reads push the written lines back to HBM before the next launch, so that launch
+    starts with an L2 of clean lines that hold none of its data and pays for no write-back of the
+    flush itself (a flush by writing alone leaves up to the L2's size of dirty lines, whose write-back
+    would be charged to the kernel timed next)."""
+
+    def __init__(self, device="cuda"):
+        import torch
+        self.w = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
+        self.r = torch.zeros(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
+        self.out = torch.empty((), dtype=torch.float32, device=device)
+
+    def __call__(self):
+        import torch
+        self.w.zero_()
+        torch.sum(self.r, dim=0, out=self.out)
+
+
 @dataclass
 class Problem:
     perm: list
@@ -90,7 +109,8 @@ TARGET_IN_FLIGHT = 18 * 1024 * 1024  # the planner's target for the bytes of til
 def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
     """Up to k (stages, ctas_per_sm) pairs other than the planner's own for a staged-kernel tile,
     nearest the planner's in-flight target first (W = CTAs x (stages - 1) x tile bytes), skipping
-    rings that would not fit the kernel's shared memory."""
+    rings that would not fit the kernel's shared memory; then the fixed round-robin tile order, and
+    shifted A runs where A's runs are too short or misaligned for the planner's 16-byte copies."""
     t = desc.get("tile") or {}
     if desc["kernel"] != "tile" or k <= 0 or not t.get("P"):
         return []
@@ -111,8 +131,12 @@ def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
             W = c * SMS * (S - 1) * tile_bytes
             # fewer CTAs than fit cost the sweep 2-12%, so they come after every full-occupancy ring
             opts.append((c != cmax(S), abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
-    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]]
-    return out + [{"round_robin": 1}]
+    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]] + [{"round_robin": 1}]
+    vm = 16 // ea if ea < 16 else 0
+    if vm and desc.get("vecA", vm) < vm and t.get("LA", 0) >= 2 * vm:
+        # A runs that 16-byte copies cannot reach directly, copied as covering 16-byte chunks
+        out.append({"shifted_runs": 1})
+    return out
 
 
 def fused_groups(p: Problem):
@@ -282,10 +306,10 @@ class Bench:
         self.B0 = torch.rand(nb, dtype=tmap[tb], device="cuda", generator=g)
         self.B = self.B0.clone()
         self.ref = None
-        self.flush_buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+        self.flush_buf = L2Flush()
 
     def flush(self):
-        self.flush_buf.zero_()
+        self.flush_buf()
 
     def run_once(self, plan: Plan):
         self.B.copy_(self.B0)

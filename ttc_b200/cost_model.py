@@ -344,9 +344,11 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
     problems when `groups` gives each row's problem)."""
     import torch
     rng = np.random.default_rng(seed)
+    val_groups = np.zeros(0, np.int64)
     if groups is not None:
         ug = rng.permutation(np.unique(groups))
-        held = np.isin(groups, ug[: int(len(ug) * val)])
+        val_groups = ug[: int(len(ug) * val)]
+        held = np.isin(groups, val_groups)
         vi, ti = np.nonzero(held)[0], rng.permutation(np.nonzero(~held)[0])
         nval = len(vi)
     else:
@@ -354,6 +356,7 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
         nval = int(len(X) * val)
         vi, ti = idx[:nval], idx[nval:]
     m = MLP(X.shape[1], 128, seed)
+    m.val_groups = val_groups
     m.mu = X[ti].mean(0)
     m.sd = X[ti].std(0) + 1e-6
     m.ymu, m.ysd = float(y[ti].mean()), float(y[ti].std() + 1e-6)
@@ -386,16 +389,6 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
 
 
 # ------------------------------------------------------------------------------------------------
-def fallback_set(order: np.ndarray, default: int, topk: int) -> list:
-    """Candidates a low-confidence selection times: the network's best topk - 1 and the planner's
-    default schedule (its top topk when the default is among them), so that a doubtful prediction
-    is checked against the method without the network."""
-    head = [int(i) for i in order[: max(topk - 1, 1)]]
-    if default in head or default < 0:
-        return [int(i) for i in order[:topk]]
-    return head + [int(default)]
-
-
 def default_index(tunings: list) -> int:
     """Position of the planner's default schedule (the empty tuning) among candidate tunings."""
     for i, tu in enumerate(tunings):
@@ -422,33 +415,62 @@ def load_default(path: Optional[Path] = None) -> MLP:
     return _loaded[str(path)]
 
 
+# The selection policy. The planner's default is within a few percent of the exhaustive search's
+# winner for most problems, so the network's top-1 is only taken on a predicted gain over the default:
+# at least POLICY["hi"] (log GB/s) untimed; between POLICY["lo"] and POLICY["hi"] the top-1 and the
+# default are timed and the faster kept; below POLICY["lo"] the default stays. `train` fits the two
+# thresholds on its held-out problems and stores them with the model.
+DEFAULT_POLICY = {"lo": 0.02, "hi": 0.3}
+
+
+def policy_of(model) -> dict:
+    return dict(DEFAULT_POLICY, **(getattr(model, "meta", {}) or {}).get("policy", {}))
+
+
+def decide(pred: np.ndarray, default: int, policy: dict) -> tuple[list, bool]:
+    """(candidate indices to use, timed?) for one problem's predictions under the policy: one index
+    when the choice is made without timing, two (top-1 and default) when they are to be timed."""
+    top = int(np.argmax(pred))
+    if default < 0:
+        return [top], False
+    if top == default:
+        return [default], False
+    gain = float(pred[top] - pred[default])
+    if gain >= policy["hi"]:
+        return [top], False
+    if gain >= policy["lo"]:
+        return [top, default], True
+    return [default], False
+
+
 def select(p: Problem, max_impl: int = 64, confidence: Optional[float] = None, verify: bool = True,
-           model: Optional[MLP] = None, topk: int = 2, measure_choice: bool = True) -> dict:
-    """Picks a schedule with the model. Below the confidence threshold, measures the network's
-    top-(k-1) predictions and the planner's default schedule and keeps the fastest (a short
-    measured search). Returns the measured results."""
+           model: Optional[MLP] = None, measure_choice: bool = True) -> dict:
+    """Picks a schedule with the model under its policy (see DEFAULT_POLICY); `confidence=0.0` takes
+    the network's top-1 untimed whatever it predicts. Returns the measured results of the timed
+    candidates (or of the choice, with measure_choice)."""
     model = model or load_default()
-    thr = 0.1 if confidence is None else confidence
     t0 = time.perf_counter()
     cands = candidate_tunings(p, max_impl, with_desc=True)
     X = features(p, cands)
     pred = model.predict(X)
     order = np.argsort(-pred)
     conf = confidence_of(pred, model.rmse)
-    fallback = conf < thr
-    picks = fallback_set(order, default_index([c[0] for c in cands]), topk) if fallback else [int(order[0])]
+    d = default_index([c[0] for c in cands])
+    if confidence == 0.0:
+        picks, timed = [int(order[0])], False
+    else:
+        picks, timed = decide(pred, d, policy_of(model))
     chosen = [cands[i][0] for i in picks]
     t_model = time.perf_counter() - t0
-    results = measure(p, chosen, reps=3, verify=verify) if (measure_choice or fallback) else []
-    return {"results": results, "confidence": conf, "fallback": fallback, "pred": pred, "order": order,
-            "candidates": cands, "seconds_model": t_model, "seconds": time.perf_counter() - t0}
+    results = measure(p, chosen, reps=3, verify=verify) if (measure_choice or timed) else []
+    return {"results": results, "confidence": conf, "fallback": timed, "pred": pred, "order": order,
+            "picks": picks, "candidates": cands, "seconds_model": t_model, "seconds": time.perf_counter() - t0}
 
 
-def fresh_head_to_head(cases: list[dict], model: Optional[MLP] = None, max_impl: int = 64, reps: int = 5,
-                       threshold: float = 0.1, topk: int = 2) -> dict:
+def fresh_head_to_head(cases: list[dict], model: Optional[MLP] = None, max_impl: int = 64, reps: int = 5) -> dict:
     """The selector against the method without it, on fresh timings: per problem, every candidate
     is timed (the exhaustive search, TTC's method), then the search's winner, the network's top-1,
-    the selector's choice (top-1 when confident, else the faster of its top-(k-1) and the default,
+    the selector's choice (under the model's policy: the default, the top-1, or the faster of the two,
     timed) and the planner default are re-timed alternately, so the winner loses the bias of being the
     maximum of noisy timings. Returns the mean shares of the winner's GB/s and the tuning times."""
     from .autotune import search
@@ -458,10 +480,10 @@ def fresh_head_to_head(cases: list[dict], model: Optional[MLP] = None, max_impl:
         p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
         sr = search(p, max_impl=max_impl, reps=3, verify=False)
         top = select(p, max_impl=max_impl, confidence=0.0, model=model, verify=False, measure_choice=False)
-        sel = select(p, max_impl=max_impl, confidence=threshold, topk=topk, model=model, verify=False,
-                     measure_choice=False)
+        sel = select(p, max_impl=max_impl, model=model, verify=False, measure_choice=False)
         top1 = top["candidates"][int(top["order"][0])][0]
-        chosen = min(sel["results"], key=lambda r: r.time_ms).tuning if sel["results"] else top1
+        chosen = (min(sel["results"], key=lambda r: r.time_ms).tuning if sel["results"]
+                  else sel["candidates"][sel["picks"][0]][0])
         picks = [sr["best"].tuning, top1, chosen, {}]
         bench = Bench(p, seed=1)
         best_ms = [float("inf")] * len(picks)
@@ -493,14 +515,14 @@ HELDOUT_SEED = 12345
 
 
 def choose_tuning(p: Problem, model: Optional[MLP] = None) -> Optional[dict]:
-    """The learned selector's schedule for one problem, as the benchmark uses it: the network's
-    top-1, or - below its confidence threshold - the faster of that and the planner default (timed
-    on the GPU with the problem's own inputs). None means the planner default."""
+    """The learned selector's schedule for one problem, as the benchmark uses it: under the model's
+    policy, the planner default, the network's top-1, or the faster of the two (timed on the GPU with
+    the problem's own inputs). None means the planner default."""
     sel = select(p, verify=False, measure_choice=False, model=model)
     if sel["results"]:
         tu = min(sel["results"], key=lambda r: r.time_ms).tuning
     else:
-        tu = sel["candidates"][int(sel["order"][0])][0]
+        tu = sel["candidates"][sel["picks"][0]][0]
     return tu or None
 
 
@@ -560,81 +582,71 @@ def _save_corpus(out: Path, d: dict):
              meta=np.frombuffer(json.dumps(d["meta"]).encode(), np.uint8))
 
 
-def stored_selection(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: dict, rmse: float,
-                     threshold: float, topk: int) -> dict:
+def stored_selection(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: dict, policy: dict) -> dict:
     """Selection quality on stored exhaustive measurements: per problem, the GB/s of the model's
-    top-1 (or, when its confidence is below the threshold, the best of the timed fallback set: its
-    top-(k-1) and the default) and of the planner's default schedule, over the best measured GB/s."""
+    top-1, of the policy's choice (when it times the top-1 and the default, the faster by the stored
+    timings) and of the planner's default schedule, each over the best measured GB/s."""
     index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
     top1, gated, dflt, fb = [], [], [], []
     for k in np.unique(case):
         rows = np.nonzero(case == k)[0]
         tunings = meta["tunings"][index_of[int(k)]]
         best = y[rows].max()
-        order = np.argsort(-pred[rows])
-        top1.append(np.exp(y[rows[order[0]]] - best))
-        low = confidence_of(pred[rows], rmse) < threshold
-        fb.append(low)
+        top1.append(np.exp(y[rows[int(np.argmax(pred[rows]))]] - best))
         d = tunings.index({}) if {} in tunings else 0
-        gated.append(np.exp(y[rows[fallback_set(order, d, topk)]].max() - best) if low else top1[-1])
+        picks, timed = decide(pred[rows], d, policy)
+        fb.append(timed)
+        gated.append(np.exp(y[rows[picks]].max() - best))
         dflt.append(np.exp(y[rows[d]] - best))
     top1, gated, dflt = map(np.asarray, (top1, gated, dflt))
     return {"cases": int(len(top1)), "top1_over_best": float(top1.mean()),
             "top1_within_5pct": float(np.mean(top1 >= 0.95)), "gated_over_best": float(gated.mean()),
-            "gated_within_5pct": float(np.mean(gated >= 0.95)), "fallback_fraction": float(np.mean(fb)),
+            "gated_within_5pct": float(np.mean(gated >= 0.95)), "timed_fraction": float(np.mean(fb)),
             "default_over_best": float(dflt.mean()), "default_within_5pct": float(np.mean(dflt >= 0.95)),
-            "gain_over_default": float(np.mean(top1 / dflt))}
+            "gain_over_default": float(np.mean(gated / dflt))}
 
 
-def evaluate(model: MLP, corpus: Path, log=print, threshold: float = 0.1, topk: int = 2, time_cases: int = 100,
-             fresh_cases: int = 100, fresh_reps: int = 10) -> dict:
+def fit_policy(pred: np.ndarray, y: np.ndarray, case: np.ndarray, meta: dict, timing_cost: float = 0.005) -> dict:
+    """The policy thresholds that keep the largest share of the best GB/s on these problems, less
+    `timing_cost` per problem that is timed (the policy's tuning time)."""
+    best, best_score = dict(DEFAULT_POLICY), -1e9
+    for lo in (0.0, 0.01, 0.02, 0.05, 0.1, 0.2, float("inf")):
+        for hi in (0.05, 0.1, 0.2, 0.3, 0.5, 1.0, float("inf")):
+            if hi < lo:
+                continue
+            pol = {"lo": lo, "hi": hi}
+            r = stored_selection(pred, y, case, meta, pol)
+            score = r["gated_over_best"] - timing_cost * r["timed_fraction"]
+            if score > best_score + 1e-9:
+                best, best_score = pol, score
+    return best
+
+
+def evaluate(model: MLP, corpus: Path, log=print, time_cases: int = 100, fresh_cases: int = 40) -> dict:
     """Held-out evaluation.
 
-    1. Stored measurements (every held-out problem): model top-1, model with its measured fallback,
-       and the planner default, each over the best GB/s of the exhaustive search.
-    2. Fresh head to head (first `fresh_cases` problems): the exhaustive search's winner, the
-       model's top-1 and the default are timed again, alternately, so that the search's winner
-       loses the selection bias of being the maximum of noisy timings.
+    1. Stored measurements (every held-out problem): the model's top-1, the policy's choice and the
+       planner default, each over the best GB/s of the exhaustive search, and the same for a grid of
+       policy thresholds.
+    2. Fresh head to head (first `fresh_cases` problems, fresh_head_to_head): the search is run
+       again and its winner, the top-1, the policy's choice and the default re-timed alternately.
     3. Tuning time (first `time_cases` problems): the exhaustive search's recorded wall time
-       against the model's (candidate planning, features, GPU inference, and the top-k timings
-       when it falls back)."""
+       against the model's (candidate planning, features, GPU inference, and the two timings when
+       the policy times)."""
     z = np.load(corpus)
     y, case = z["y"], z["case"]
     meta = json.loads(bytes(z["meta"]).decode())
     X, _ = corpus_features(meta)
     pred = model.predict(X)
-    res = {"stored": {"threshold": threshold, "topk": topk,
-                      **stored_selection(pred, y, case, meta, model.rmse, threshold, topk)},
-           "stored_curve": [dict(threshold=t, topk=kk, **{k: v for k, v in stored_selection(
-               pred, y, case, meta, model.rmse, t, kk).items() if k in ("gated_over_best", "fallback_fraction")})
-                            for t in (0.0, 0.05, 0.1, 0.2, 0.35) for kk in (2, 4)]}
-    index_of = {int(c["index"]): i for i, c in enumerate(meta["cases"])}
+    pol = policy_of(model)
+    res = {"policy": pol, "stored": stored_selection(pred, y, case, meta, pol),
+           "stored_curve": [dict(lo=lo, hi=hi, **{k: v for k, v in stored_selection(
+               pred, y, case, meta, {"lo": lo, "hi": hi}).items() if k in ("gated_over_best", "timed_fraction")})
+                            for lo in (0.0, 0.02, 0.05, 0.1) for hi in (0.1, 0.3, 1.0)]}
     cases = meta["cases"]
     search_s = z["search_s"]
-
-    # fresh head to head
-    h2h = []
-    for c in cases[:fresh_cases]:
-        k = int(c["index"])
-        rows = np.nonzero(case == k)[0]
-        tunings = meta["tunings"][index_of[k]]
-        p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
-        picks = [tunings[int(np.argmax(y[rows]))], tunings[int(np.argmax(pred[rows]))], {}]
-        bench = Bench(p, seed=k)
-        best_ms = [float("inf")] * 3
-        for rnd in range(2):
-            order = [0, 1, 2] if rnd == 0 else [2, 1, 0]
-            res_r = measure(p, [picks[i] for i in order], reps=fresh_reps, verify=False, bench=bench)
-            for i, r in zip(order, res_r):
-                best_ms[i] = min(best_ms[i], r.time_ms)
-        del bench
-        h2h.append([best_ms[0] / best_ms[1], best_ms[0] / best_ms[2]])
-    if h2h:
-        h = np.asarray(h2h)
-        res["fresh"] = {"cases": int(len(h)), "reps": fresh_reps, "model_over_search": float(h[:, 0].mean()),
-                        "model_within_5pct": float(np.mean(h[:, 0] >= 0.95)),
-                        "default_over_search": float(h[:, 1].mean()),
-                        "default_within_5pct": float(np.mean(h[:, 1] >= 0.95))}
+    if fresh_cases:
+        res["fresh"] = fresh_head_to_head(cases[:fresh_cases], model)
 
     # tuning time
     t_top1, t_gated, t_search, fbs = [], [], [], 0
@@ -642,16 +654,16 @@ def evaluate(model: MLP, corpus: Path, log=print, threshold: float = 0.1, topk: 
         p = Problem(c["perm"], c["size"], c["dtype"], c.get("alpha", 1.0), c.get("beta", 0.0))
         r = select(p, confidence=0.0, model=model, verify=False, measure_choice=False)
         t_top1.append(r["seconds"])
-        r = select(p, confidence=threshold, model=model, topk=topk, verify=False, measure_choice=False)
+        r = select(p, model=model, verify=False, measure_choice=False)
         t_gated.append(r["seconds"])
         fbs += int(r["fallback"])
         t_search.append(search_s[i])
     res["time"] = {"cases": len(t_search), "search_seconds_mean": float(np.mean(t_search)),
                    "model_top1_seconds_mean": float(np.mean(t_top1)),
-                   "model_gated_seconds_mean": float(np.mean(t_gated)),
+                   "model_policy_seconds_mean": float(np.mean(t_gated)),
                    "top1_speedup": float(np.mean(t_search) / max(np.mean(t_top1), 1e-9)),
-                   "gated_speedup": float(np.mean(t_search) / max(np.mean(t_gated), 1e-9)),
-                   "gated_fallbacks": fbs}
+                   "policy_speedup": float(np.mean(t_search) / max(np.mean(t_gated), 1e-9)),
+                   "policy_timed": fbs}
     res["rmse"] = model.rmse
     if log:
         log(json.dumps(res, indent=1))
@@ -669,8 +681,6 @@ def main(argv=None):
     ap.add_argument("--model", default=str(DEFAULT_MODEL))
     ap.add_argument("--max-impl", type=int, default=64)
     ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--threshold", type=float, default=0.1)
-    ap.add_argument("--topk", type=int, default=2)
     ap.add_argument("--out-json", default=None)
     ap.add_argument("--max-seconds", type=float, default=None, help="collect: stop (resumably) after this long")
     a = ap.parse_args(argv)
@@ -683,13 +693,17 @@ def main(argv=None):
     elif a.cmd == "train":
         z = np.load(train_path)
         X, case = corpus_features(json.loads(bytes(z["meta"]).decode()))
+        meta = json.loads(bytes(z["meta"]).decode())
         m = train(X, z["y"], epochs=a.epochs, groups=case)
+        # the policy thresholds, fitted on the training run's held-out problems
+        held = np.isin(case, m.val_groups)
+        policy = fit_policy(m.predict(X[held]), z["y"][held], case[held], meta) if held.any() else DEFAULT_POLICY
         digest = hashlib.sha256(z["X"].tobytes()[:1 << 20]).hexdigest()[:16]
-        m.save(Path(a.model), {"trained_rows": int(len(z["y"])), "corpus_digest": digest})
-        print(f"saved {a.model} (val rmse {m.rmse:.4f})")
+        m.save(Path(a.model), {"trained_rows": int(len(z["y"])), "corpus_digest": digest, "policy": policy})
+        print(f"saved {a.model} (val rmse {m.rmse:.4f}, policy {policy})")
     else:
         m = MLP.load(Path(a.model))
-        res = evaluate(m, test_path, threshold=a.threshold, topk=a.topk)
+        res = evaluate(m, test_path)
         if a.out_json:
             Path(a.out_json).write_text(json.dumps(res, indent=1))
 

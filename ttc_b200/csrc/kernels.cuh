@@ -760,7 +760,15 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       default: cp_async_wait<5>(); break;
     }
     __syncthreads();
-    if constexpr (!DYN) {
+    if constexpr (DYN) {
+      // the tile of iteration k + D + 2 (read after the next barrier), and the next claim, whose
+      // result thread 0 needs only an iteration later (decoding here, before thread 0's own stores,
+      // timed 3% faster over the 200 MiB sweep than after them)
+      if (tid == 0) {
+        decode_into(pending, info[(k + D + 2) % kInfoRing]);
+        pending = atomicAdd(&sched[0], 1u);
+      }
+    } else {
       const uint32_t t = blockIdx.x + k * G;
       if (tid < kDecodeBatch && k % kDecodeBatch == 0 && k != 0)
         decode_into(t + (kDecodeBatch + tid) * G, info[(k + kDecodeBatch + tid) % kInfoRing]);
@@ -811,14 +819,6 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
             out_vec(stage, sB, q, off, Bt + (segB[s] + (q - s * LB)));
           }
         }
-      }
-    }
-    if constexpr (DYN) {
-      // after its own stores, thread 0 decodes the tile of iteration k + D + 2 (read after the next
-      // barrier) and sends the next claim, whose result it needs only an iteration later
-      if (tid == 0) {
-        decode_into(pending, info[(k + D + 2) % kInfoRing]);
-        pending = atomicAdd(&sched[0], 1u);
       }
     }
     cur = cur + 1 == S ? 0 : cur + 1;
