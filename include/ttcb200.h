@@ -84,12 +84,16 @@ typedef struct {
                             copies in flight); 0 = planner's choice                             */
   int32_t ctas_per_sm;   /* staged tile kernel: resident CTAs per SM (1..8, capped by what fits);
                             0 = planner's choice. `blocks`, when set, takes precedence          */
-  int32_t round_robin;   /* staged tile kernel: 0 = CTAs claim tiles in order from a counter the
-                            plan owns, 1 = fixed round-robin order (tile blockIdx + k * CTAs)    */
+  int32_t round_robin;   /* staged tile kernel: 0 = planner's choice (the round-robin order),
+                            1 = fixed round-robin order (tile blockIdx + k * CTAs), -1 = CTAs
+                            claim tiles in order from counters the plan owns                    */
   int32_t shifted_runs;  /* staged tile kernel: 1 = copy A runs that 16-byte accesses cannot
                             reach directly (odd lengths or offsets) as the 16-byte chunks that
                             cover them; 0 = planner's choice (plain copies), -1 = never         */
-  int32_t reserved[1];
+  int32_t bulk_copies;   /* staged tile kernel: 1 = move each A run with one bulk copy
+                            (cp.async.bulk into the stage, completion counted on an mbarrier)
+                            where the runs allow it (16-byte aligned runs, or shifted runs);
+                            0 = planner's choice (per-thread 16-byte copies), -1 = never       */
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;
@@ -113,10 +117,10 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
  * plan created with beta_nonzero == 0. */
 ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const void* alpha,
                            const void* beta, ttcb_stream_t stream);
-/* Calls with one plan may overlap on the GPU (several streams): its staged kernel takes the counter
- * words it claims tiles from in turn from 64 slot pairs, so up to 64 launches of one plan can be in
- * flight at once. A launch captured in a CUDA graph keeps its slot; replays of that graph must not
- * overlap each other. */
+/* Calls with one plan may overlap on the GPU (several streams). A plan whose schedule claims tiles
+ * from counters (round_robin = -1) takes the counter words in turn from 64 slot pairs, so up to 64
+ * of its launches can be in flight at once; a launch captured in a CUDA graph keeps its slot, and
+ * replays of that graph must not overlap each other. */
 
 /* Allocation-free transposition, for callers that may not allocate device memory (their memory is
  * owned by an external pool, or cudaMalloc is forbidden where they run). It has no counterpart in
@@ -144,6 +148,13 @@ size_t ttcb_plan_describe(const ttcb_plan* plan, char* buf, size_t len);
 /* Algorithmic bytes of one call: N*(sizeof(TA) + sizeof(TB)*(1 + [beta != 0])), N = prod size,
  * the bandwidth convention of GPUtransposeGenerator.py:589-592 (padding excluded). */
 int64_t ttcb_plan_bytes(const ttcb_plan* plan);
+
+/* Stage waits of the plan's staged kernel that ran out of time since the plan was created or last
+ * asked (a plan with bulk A copies waits on its stage barriers with a limit of 2 s; a wait that runs
+ * out means copies never landed, and that launch left tiles of B unwritten). Writes the count and
+ * clears it; 0 for plans without bulk copies. Copies from the device, so it waits for the device's
+ * work that is ordered before it on the legacy default stream. No counterpart in TTC. */
+ttcb_status ttcb_plan_wait_timeouts(const ttcb_plan* plan, unsigned int* count);
 
 /* Message of the last failure on this thread ("" if none). Replaces ttc_util.py:135-141, which
  * printed the CUDA error and called exit(-1). */

@@ -107,8 +107,63 @@ def parse_tile(b):
     t["ptab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_perm"]).astype(np.int64)
     t["gtab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_gtab"]).astype(np.int64)
     o = L["off_shiftA"]
-    t["shiftA"], t["shiftW"], t["shiftCM"] = _i32(b, o), _i32(b, o + 4), _i32(b, o + 8)
+    t["shiftA"], t["shiftW"], t["shiftCM"], t["bulkA"] = _i32(b, o), _i32(b, o + 4), _i32(b, o + 8), _i32(b, o + 12)
     return t
+
+
+def check_bulk_layout(t, EA):
+    """Bulk A copies (one cp.async.bulk per run, warp 0's lanes): replay the copies of a tile for
+    every tile shift the kernel can meet and check that each starts and ends on 16-byte boundaries
+    of shared memory and of A (tile bases included), stays inside its stage, and that the gather at
+    gtab[q] (+ the shift) reads A element segA[s] + j of position p(q) = s*LA + j; and that the byte
+    count announced to the stage barrier equals the bytes copied."""
+    V = 16 // EA
+    P, LA = t["P"], t["LA"]
+    nseg = P // LA
+    segA = t["segA"].astype(np.int64)
+    q = np.arange(P, dtype=np.int64)
+    slot_q = q + ((q >> t["pshift"]) if t["pad"] else 0)
+    inv = np.full(t["phys_size"], -1, np.int64)
+    inv[t["ptab"]] = np.arange(P, dtype=np.int64)
+    p_of_q = inv[slot_q]
+    want = segA[p_of_q // LA] + p_of_q % LA
+    stage_bytes = ((t["stage_elems"] * EA + 15) // 16) * 16
+    if not t["shiftA"]:
+        assert t["sigmaA"] % LA == 0, "a padding point splits a run"
+        assert (LA * EA) % 16 == 0 and (segA * EA % 16 == 0).all()
+        for g in t["g"]:
+            assert (g["strideA"] * EA) % 16 == 0, "a tile base off the 16-byte grid"
+        src = np.full(stage_bytes // EA + V, -(1 << 60), np.int64)
+        total = 0
+        for s in range(nseg):
+            p = s * LA
+            dst = p + (p // t["sigmaA"]) * t["padA"]
+            assert (dst * EA) % 16 == 0 and (dst + LA) * EA <= stage_bytes
+            src[dst:dst + LA] = segA[s] + np.arange(LA)
+            total += LA * EA
+        assert total == P * EA
+        assert np.array_equal(src[t["gtab"]], want), "a gather reads an element no bulk copy brought"
+        return
+    W = t["shiftW"]
+    assert W % V == 0
+    for x in range(V):
+        src = np.full(stage_bytes // EA + 2 * V, -(1 << 60), np.int64)
+        total = 0
+        for s in range(nseg):
+            y = int(segA[s] % V)
+            clo, chi = (x + y) // V, (x + y + LA - 1) // V
+            dst = s * W + V * clo
+            first = segA[s] - y + V * clo - x  # A element (from the tile base) of the copy's first slot
+            n = (chi - clo + 1) * V
+            assert ((first + x) * EA) % 16 == 0 and (dst * EA) % 16 == 0 and (dst + n) * EA <= stage_bytes
+            # every 16-byte chunk of the copy holds an element of the run
+            for c in range(clo, chi + 1):
+                lo_el = segA[s] - y + V * c - x
+                assert lo_el + V > segA[s] and lo_el < segA[s] + LA
+            src[dst:dst + n] = first + np.arange(n)
+            total += n * EA
+        got = src[t["gtab"] + x]
+        assert np.array_equal(got, want), f"shift {x}: a gather reads an element no bulk copy brought"
 
 
 def check_shifted_layout(t, p_of_q, V):

@@ -37,6 +37,7 @@ def run_gpu(A, B, perm, size, dtype, alpha, beta, lda=None, ldb=None, tuning=Non
     tail = dB[offset + B.size:].cpu().numpy()
     assert np.array_equal(tail.view(np.uint8), canary.numpy().view(np.uint8)), "write past the end of B"
     desc = plan.describe()
+    assert plan.wait_timeouts() == 0, "a stage wait of the bulk-copy kernel ran out of time"
     plan.close()
     return out, desc
 
@@ -97,7 +98,9 @@ def test_padded_lda_ldb_and_complex_beta(dtype):
 TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"loop_order": 3}, {"blocks": 7}, {"tile_elems": 512},
            {"tile_elems": 8192}, {"run_bytes": 128}, {"run_bytes": 2048}, {"kernel": 1}, {"streaming": -1},
            {"streaming": 1}, {"round_robin": 1}, {"stages": 3}, {"stages": 7}, {"ctas_per_sm": 1},
-           {"stages": 6, "ctas_per_sm": 2}, {"round_robin": 1, "blocks": 5}]
+           {"stages": 6, "ctas_per_sm": 2}, {"round_robin": 1, "blocks": 5}, {"round_robin": -1},
+           {"round_robin": -1, "blocks": 5}, {"bulk_copies": 1}, {"bulk_copies": 1, "round_robin": -1},
+           {"bulk_copies": 1, "shifted_runs": 1}]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS, ids=[str(t) for t in TUNINGS])
@@ -340,7 +343,7 @@ def test_claimed_tiles_with_concurrent_launches_and_slot_reuse():
     import torch
     from ttc_b200 import Plan
     perm, size = [2, 0, 1], [67, 45, 311]
-    plan = Plan(perm, size, "s", True, tuning={"blocks": 16})  # many tiles per CTA: claims on
+    plan = Plan(perm, size, "s", True, tuning={"blocks": 16, "round_robin": -1})
     assert plan.describe()["tile"]["async"] == 1 and plan.describe()["tile"]["claims"] == 1
     n = int(np.prod(size))
     streams = [torch.cuda.Stream() for _ in range(4)]
@@ -371,6 +374,46 @@ SHIFTED = [([1, 0], [99, 1001]), ([1, 0, 3, 2], [99, 17, 35, 3]), ([1, 0, 2], [4
            ([2, 1, 0], [10, 25, 2097]), ([0, 2, 1], [31, 110, 15]), ([2, 0, 1], [23, 13, 240])]
 
 
+BULK = [([1, 0, 2], [300, 256, 5]), ([2, 0, 1], [8, 64, 1000]), ([1, 0], [1024, 999]), ([3, 1, 0, 2], [16, 20, 24, 9]),
+        ([1, 0, 2], [1000, 768, 16])]
+
+
+@pytest.mark.parametrize("dtype", ["s", "d", "c", "z", "sd", "ds", "zc"])
+def test_bulk_a_copies(dtype):
+    """A runs moved by one bulk copy each (cp.async.bulk into the stage, an mbarrier per stage):
+    bit for bit against the oracle for aligned runs and for shifted runs at A offsets of 0 to 3
+    elements, beta = 0 and beta != 0, round-robin and claimed tiles, the shallowest and deepest rings;
+    no stage wait runs out of time (run_gpu checks the plan's count)."""
+    used = 0
+    for perm, size in BULK + SHIFTED:
+        for beta in (0.0, -0.5):
+            desc = check_case(perm, size, dtype, 1.5, beta, tuning={"bulk_copies": 1})
+            used += int((desc.get("tile") or {}).get("bulk", 0))
+            for offset in (0, 1, 3):
+                check_case(perm, size, dtype, 1.5, beta, offset=offset, tuning={"bulk_copies": 1, "shifted_runs": 1})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"bulk_copies": 1, "round_robin": 1, "stages": 3})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"bulk_copies": 1, "blocks": 9, "stages": 7,
+                                                             "round_robin": -1})
+    assert used > 0
+
+
+def test_bounded_wait_gives_up_and_the_context_survives():
+    """The stage wait of the bulk-copy kernel has a time limit: on a barrier phase that nothing
+    completes it gives up after the limit and reports it, and the context stays usable; on a phase
+    that completes it does not give up."""
+    import ctypes
+    import time
+    from ttc_b200 import _native
+    lib = _native.lib()
+    n = ctypes.c_uint(7)
+    t0 = time.perf_counter()
+    assert lib.ttcb_test_bounded_wait(20_000_000, 0, ctypes.byref(n)) == 0
+    assert n.value == 1 and time.perf_counter() - t0 >= 0.02
+    assert lib.ttcb_test_bounded_wait(20_000_000, 1, ctypes.byref(n)) == 0
+    assert n.value == 0
+    check_case([1, 0, 2], [300, 256, 5], "s", 1.5, -0.5, tuning={"bulk_copies": 1})
+
+
 @pytest.mark.parametrize("dtype", ["s", "d", "c", "sd", "ds", "cz"])
 def test_shifted_a_runs(dtype):
     """A runs of odd lengths and offsets copied as the 16-byte chunks that cover them, shifted per
@@ -384,5 +427,5 @@ def test_shifted_a_runs(dtype):
                 used += int((desc.get("tile") or {}).get("shifted_runs", 0))
             check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": -1})
             check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 1, "round_robin": 1, "stages": 5})
-            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 1, "blocks": 9})  # claimed tiles
+            check_case(perm, size, dtype, 1.5, beta, tuning={"shifted_runs": 1, "blocks": 9, "round_robin": -1})
     assert used > 0

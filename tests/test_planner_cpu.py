@@ -84,7 +84,8 @@ def _oracle_pairs(perm, size, lda, ldb):
 
 
 TUNINGS = [None, {"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"tile_elems": 256}, {"tile_elems": 8192},
-           {"run_bytes": 128}, {"run_bytes": 1024}, {"kernel": 1}, {"shifted_runs": 1}]
+           {"run_bytes": 128}, {"run_bytes": 1024}, {"kernel": 1}, {"shifted_runs": 1}, {"bulk_copies": 1},
+           {"bulk_copies": 1, "shifted_runs": 1}]
 
 
 def test_kernel_index_math_replay_matches_oracle_mapping():
@@ -353,7 +354,7 @@ def test_search_adds_ttc_ranked_loop_orders():
     cands = candidate_tunings(p, 500, knob_space("s", ttc_orders=2), with_desc=True)
     by_shape = {}
     for tu, d in cands:
-        if d["kernel"] != "tile" or {"stages", "round_robin", "shifted_runs"} & set(tu):  # schedule alternatives reuse the first raster
+        if d["kernel"] != "tile" or {"stages", "round_robin", "shifted_runs", "bulk_copies"} & set(tu):  # schedule alternatives reuse the first raster
             continue
         key = json.dumps({k: v for k, v in tu.items() if k in ("tile_elems", "run_bytes")}, sort_keys=True)
         by_shape.setdefault(key, (d, []))[1].append(tu)
@@ -400,3 +401,35 @@ def test_shifted_a_runs_replay():
             wa, wb = _oracle_pairs(perm, size, lda, ldb)
             assert dict(zip(b.tolist(), a.tolist())) == dict(zip(wb.tolist(), wa.tolist()))
     assert shifted >= 30
+
+
+def test_bulk_copy_layout_replay():
+    """Bulk A copies (tuning bulk_copies = 1, alone and with shifted runs): for random problems, the
+    CPU replay of warp 0's bulk copies (kernel_sim.check_bulk_layout) must keep every copy on 16-byte
+    boundaries and inside its stage and bring every element the store phase gathers; plans whose runs
+    allow no bulk copy must not ask for them; and the element mapping must equal the oracle's."""
+    rng = np.random.default_rng(12)
+    seen = {0: 0, 1: 0}
+    for it in range(70):
+        perm, size, lda, ldb = _random_problem(rng, max_rank=4, max_ext=24)
+        for dtype in ("s", "d", "c", "z", "sd"):
+            for tu in ({"bulk_copies": 1}, {"bulk_copies": 1, "shifted_runs": 1}):
+                try:
+                    kind, b = kernel_sim.host_desc(perm, size, dtype, False, lda, ldb, tu)
+                except TTCError:
+                    continue
+                if kind != 1:
+                    continue
+                t = kernel_sim.parse_tile(b)
+                j = plan_host_json(perm, size, dtype, False, lda, ldb, tu)
+                EA = {"s": 4, "d": 8, "c": 8, "z": 16}[dtype[0]]
+                if not t["bulkA"]:
+                    assert not t["shiftA"] and j["vecA"] * EA != 16
+                    continue
+                seen[t["shiftA"]] += 1
+                kernel_sim.check_bulk_layout(t, EA)
+                kernel_sim.check_staged_layout(t, j["vecA"])
+                _, (a, bb) = kernel_sim.simulate(perm, size, dtype, False, lda, ldb, tu)
+                wa, wb = _oracle_pairs(perm, size, lda, ldb)
+                assert dict(zip(bb.tolist(), a.tolist())) == dict(zip(wb.tolist(), wa.tolist()))
+    assert seen[0] >= 40 and seen[1] >= 20, seen

@@ -63,7 +63,7 @@ class Tuning(ctypes.Structure):
                 ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("ragged", ctypes.c_int32),
                 ("raster_lo", ctypes.c_int32), ("raster_hi", ctypes.c_int32), ("stages", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("round_robin", ctypes.c_int32),
-                ("shifted_runs", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
+                ("shifted_runs", ctypes.c_int32), ("bulk_copies", ctypes.c_int32)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":
@@ -79,7 +79,7 @@ class Tuning(ctypes.Structure):
         return t
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "raster_lo", "raster_hi")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("raster_lo", "raster_hi")}
         if self.loop_order == 4:
             d["raster"] = unpack_raster(self.raster_lo, self.raster_hi)
         return d
@@ -98,6 +98,7 @@ PUBLIC_SYMBOLS = [
     ("ttcb_plan_destroy", None, [_P]),
     ("ttcb_plan_describe", ctypes.c_size_t, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     ("ttcb_plan_bytes", ctypes.c_int64, [_P]),
+    ("ttcb_plan_wait_timeouts", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint)]),
     ("ttcb_last_error", ctypes.c_char_p, []),
     ("ttcb_version", None, [_IP, _IP, _IP]),
     ("ttcb_batch_create", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(_P), ctypes.POINTER(_P),
@@ -112,6 +113,7 @@ PUBLIC_SYMBOLS = [
 ]
 
 TEST_SYMBOLS = [
+    ("ttcb_test_bounded_wait", ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]),
     ("ttcb_test_fuse", ctypes.c_int, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, _IP, _IP, _I64P, _I64P, _I64P]),
     ("ttcb_test_plan_host", ctypes.c_int, [ctypes.c_int, _IP, _I64P, _I64P, _I64P, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, ctypes.POINTER(Tuning), ctypes.c_char_p, ctypes.c_size_t]),

@@ -109,8 +109,9 @@ TARGET_IN_FLIGHT = 18 * 1024 * 1024  # the planner's target for the bytes of til
 def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
     """Up to k (stages, ctas_per_sm) pairs other than the planner's own for a staged-kernel tile,
     nearest the planner's in-flight target first (W = CTAs x (stages - 1) x tile bytes), skipping
-    rings that would not fit the kernel's shared memory; then the fixed round-robin tile order, and
-    shifted A runs where A's runs are too short or misaligned for the planner's 16-byte copies."""
+    rings that would not fit the kernel's shared memory; then tiles claimed in order from counters,
+    bulk A copies where 16-byte vectors reach A's runs, and otherwise shifted A runs (with per-thread
+    or bulk copies) where the runs are long enough."""
     t = desc.get("tile") or {}
     if desc["kernel"] != "tile" or k <= 0 or not t.get("P"):
         return []
@@ -131,11 +132,13 @@ def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
             W = c * SMS * (S - 1) * tile_bytes
             # fewer CTAs than fit cost the sweep 2-12%, so they come after every full-occupancy ring
             opts.append((c != cmax(S), abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
-    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]] + [{"round_robin": 1}]
-    vm = 16 // ea if ea < 16 else 0
-    if vm and desc.get("vecA", vm) < vm and t.get("LA", 0) >= 2 * vm:
+    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]] + [{"round_robin": -1}]
+    vm = 16 // ea
+    if desc.get("vecA", vm) * ea == 16:
+        out.append({"bulk_copies": 1})
+    elif t.get("LA", 0) >= 2 * vm:
         # A runs that 16-byte copies cannot reach directly, copied as covering 16-byte chunks
-        out.append({"shifted_runs": 1})
+        out += [{"shifted_runs": 1}, {"shifted_runs": 1, "bulk_copies": 1}]
     return out
 
 

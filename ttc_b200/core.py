@@ -121,6 +121,13 @@ class Plan:
         """Kernels one call launches (with 16-byte aligned tensors): see `describe_launches`."""
         return describe_launches(self.describe())
 
+    def wait_timeouts(self) -> int:
+        """Stage waits of the staged kernel's bulk-copy form that ran out of time since the last
+        query (0 when every launch's copies landed); reading clears the count."""
+        n = ctypes.c_uint(0)
+        check(lib().ttcb_plan_wait_timeouts(self._h, ctypes.byref(n)))
+        return int(n.value)
+
     @property
     def bytes(self) -> int:
         """Algorithmic bytes per call: N*(|TA| + |TB|*(1+[beta!=0]))."""

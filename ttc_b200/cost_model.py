@@ -34,7 +34,7 @@ from .core import ELEM_BYTES, plan_shapes, split_dtype
 
 MAXD = 6
 DEFAULT_MODEL = Path(__file__).resolve().parent / "data" / "cost_model.npz"
-VERSION = "ttcb-mlp-v3"
+VERSION = "ttcb-mlp-v4"
 
 
 # ------------------------------------------------------------------------------------------------
@@ -140,6 +140,9 @@ def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None, groups=
                 1.0 if bl == 0 else 0.0, bl / 444.0, S / 6.0, c / 4.0, math.log2(max(W, 1)) / 30.0] + mid
     waves = nt / ctas
     f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves)] + tail
+    # how the staged kernel moves the tiles: claimed in order or round robin; A runs shifted; bulk copies
+    f += [1.0 if tuning.get("round_robin", 0) == -1 else 0.0, float(t.get("shifted_runs", 0)),
+          float(t.get("bulk", 0))]
     f += _raster_jumps(p, tuning, desc, groups)
     return f
 

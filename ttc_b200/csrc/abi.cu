@@ -86,10 +86,20 @@ unsigned int* plan_claim_slot(const ttcb_plan* p) {
 using ttcb::allow_large_smem;
 using ttcb::needs_large_smem;
 
-// The staged kernel claims tiles from the plan's counters unless the schedule asks for the fixed
-// round-robin order or the plan has none.
-static bool uses_claims(const ttcb_plan* p) { return p->claim_words && p->tuning.round_robin != 1; }
-static constexpr int kClaimMinTilesPerCta = 16;
+// The staged kernel claims tiles from the plan's counters when the schedule asks for it
+// (round_robin = -1, and the plan then has counters); otherwise it takes the round-robin order.
+static bool uses_claims(const ttcb_plan* p) { return p->claim_words != nullptr; }
+// The staged kernel moves A runs with bulk copies when the plan's layout allows it and A's pointer
+// meets the layout's alignment (shifted runs take any pointer; plain runs need the 16-byte vector).
+static bool uses_bulk(const ttcb_plan* p, const TileDesc* td, int va, int EA) {
+  return td->bulkA && p->wait_status && (td->shiftA || va * EA == 16);
+}
+static int staged_kernel_id(const ttcb_plan* p, const TileDesc* td, bool reg, bool bulk) {
+  const bool claims = uses_claims(p);
+  const int k = reg ? (claims ? TTCB_KERNEL_TILE_ASYNC_REG_DYN : TTCB_KERNEL_TILE_ASYNC_REG)
+                    : (claims ? TTCB_KERNEL_TILE_ASYNC_DYN : TTCB_KERNEL_TILE_ASYNC);
+  return bulk ? (k | TTCB_KERNEL_BULK_FLAG) : k;
+}
 
 static ttcb_status plan_finish_device(ttcb_plan* p) {
   if (p->empty) return TTCB_OK;
@@ -124,9 +134,7 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
     if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) return fail(TTCB_ERR_UNSUPPORTED, "tile does not fit in shared memory");
     // the staged kernel's schedule may ask for fewer CTAs per SM than fit (see the planner)
-    if ((kernel_id == TTCB_KERNEL_TILE_ASYNC || kernel_id == TTCB_KERNEL_TILE_ASYNC_REG ||
-         kernel_id == TTCB_KERNEL_TILE_ASYNC_DYN || kernel_id == TTCB_KERNEL_TILE_ASYNC_REG_DYN) &&
-        p->ctas_per_sm > 0)
+    if (ttcb_is_staged_kernel(kernel_id) && p->ctas_per_sm > 0)
       per_sm = std::min(per_sm, p->ctas_per_sm);
     int64_t resident = (int64_t)per_sm * sms;
     int64_t blocks;
@@ -152,14 +160,11 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (s != TTCB_OK) return s;
     }
     if (td->async_ok) {
-      // Tiles are claimed in order only when every CTA has many of them (a problem of 200 MiB has
-      // 20 to 150 per CTA): the claims helped the 200 MiB sweep by about 1%, but a CTA claims its
-      // first S tiles at once, which on problems of a few tiles per CTA leaves most CTAs idle (1 to
-      // 4 MiB problems lost a quarter of their speed).
-      s = grid_for(td->reg_ok ? TTCB_KERNEL_TILE_ASYNC_REG : TTCB_KERNEL_TILE_ASYNC, p->smem_async,
-                   &p->blocks_async, td->nfull);
-      if (s != TTCB_OK) return s;
-      if (p->tuning.round_robin != 1 && td->nfull >= (int64_t)kClaimMinTilesPerCta * p->blocks_async) {
+      // Tiles are claimed in order from counters only when the schedule asks for it: timed over the
+      // 200 MiB sweep back to back the claims were 0.5-1% slower than the round-robin order and on
+      // the 147 MB 1000x768x16 transposition 15% slower; and a CTA claims its first S tiles at once,
+      // which on problems of a few tiles per CTA leaves most CTAs idle.
+      if (p->tuning.round_robin == -1) {
         e = cudaMalloc(&p->claim_words, sizeof(unsigned int) * 2 * ttcb::kClaimSlots);
         if (e != cudaSuccess) {
           p->claim_words = nullptr;
@@ -171,10 +176,19 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
         p->launch_count = new (std::nothrow) std::atomic<unsigned int>(0);
         if (!p->launch_count) return fail(TTCB_ERR_ALLOC, "host allocation of the launch counter failed");
       }
-      const bool claims = uses_claims(p);
-      s = grid_for(td->reg_ok ? (claims ? TTCB_KERNEL_TILE_ASYNC_REG_DYN : TTCB_KERNEL_TILE_ASYNC_REG)
-                              : (claims ? TTCB_KERNEL_TILE_ASYNC_DYN : TTCB_KERNEL_TILE_ASYNC),
-                   p->smem_async, &p->blocks_async, td->nfull);
+      if (td->bulkA) {
+        e = cudaMalloc(&p->wait_status, sizeof(unsigned int));
+        if (e != cudaSuccess) {
+          p->wait_status = nullptr;
+          cudaGetLastError();
+          return fail(TTCB_ERR_ALLOC, std::string("cudaMalloc of the wait status failed: ") + cudaGetErrorString(e));
+        }
+        if ((e = cudaMemset(p->wait_status, 0, sizeof(unsigned int))) != cudaSuccess)
+          return cuda_fail(e, "cudaMemset of the wait status");
+      }
+      const int EA = dtype_bytes(p->ta);
+      s = grid_for(staged_kernel_id(p, td, td->reg_ok, uses_bulk(p, td, p->vecA, EA)), p->smem_async, &p->blocks_async,
+                   td->nfull);
       if (s != TTCB_OK) return s;
       if (td->nrag0 + td->nrag1 > 0) {
         s = grid_for(TTCB_KERNEL_TILE_RAGGED, p->smem_ragged, &p->blocks_ragged, (int64_t)td->nrag0 + td->nrag1);
@@ -223,9 +237,7 @@ static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const
     if (shifted && !((want == 0 || want == 3) && td->async_ok))
       return fail(TTCB_ERR_UNSUPPORTED, "a plan with shifted A runs runs only on the staged tile kernel");
     if ((want == 0 || want == 3) && td->async_ok) {
-      const bool claims = uses_claims(p);
-      kernel = (fast_ok && td->reg_ok) ? (claims ? TTCB_KERNEL_TILE_ASYNC_REG_DYN : TTCB_KERNEL_TILE_ASYNC_REG)
-                                       : (claims ? TTCB_KERNEL_TILE_ASYNC_DYN : TTCB_KERNEL_TILE_ASYNC);
+      kernel = staged_kernel_id(p, td, fast_ok && td->reg_ok, uses_bulk(p, td, va, EA));
       blocks = p->blocks_async;
       smem = p->smem_async;
     } else if ((want == 0 || want == 2) && fast_ok) {
@@ -238,9 +250,7 @@ static ttcb_status launch_plan(const ttcb_plan* p, const void* A, void* B, const
   if (!k.fn) return fail(TTCB_ERR_DTYPE, "no kernel for this type pair");
   if (needs_large_smem(smem)) allow_large_smem(k.func);
   const TileDesc* td = reinterpret_cast<const TileDesc*>(p->host_desc.data());
-  const bool ragged = (kernel == TTCB_KERNEL_TILE_ASYNC || kernel == TTCB_KERNEL_TILE_ASYNC_REG ||
-                       kernel == TTCB_KERNEL_TILE_ASYNC_DYN || kernel == TTCB_KERNEL_TILE_ASYNC_REG_DYN) &&
-                      td->nrag0 + td->nrag1 > 0;
+  const bool ragged = ttcb_is_staged_kernel(kernel) && td->nrag0 + td->nrag1 > 0;
   if (!ragged) {
     e = k.fn(p, A, B, alpha, beta, st, blocks);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -382,6 +392,7 @@ void ttcb_plan_destroy(ttcb_plan* plan) {
   for (int k = 0; k < plan->nedge; ++k) ttcb_plan_destroy(plan->edge[k]);
   if (plan->dev_desc) cudaFree(plan->dev_desc);
   if (plan->claim_words) cudaFree(plan->claim_words);
+  if (plan->wait_status) cudaFree(plan->wait_status);
   delete static_cast<std::atomic<unsigned int>*>(plan->launch_count);
   if (plan->side_stream) cudaStreamDestroy(static_cast<cudaStream_t>(plan->side_stream));
   if (plan->ev_fork) cudaEventDestroy(static_cast<cudaEvent_t>(plan->ev_fork));
@@ -418,6 +429,50 @@ size_t ttcb_plan_describe(const ttcb_plan* plan, char* buf, size_t len) {
     buf[n] = 0;
   }
   return s.size() + 1;
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void bounded_wait_kernel(uint64_t limit_ns, int arrive, unsigned int* gave_up) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = ttcb::smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    ttcb::mbar_init(b, 1);
+    ttcb::mbar_fence_init();
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) ttcb::mbar_arrive(b);
+  const bool done = ttcb::mbar_wait_bounded(b, 0, limit_ns);
+  if (__syncthreads_or(!done) && threadIdx.x == 0) atomicAdd(gave_up, 1u);
+}
+}  // namespace
+
+extern "C" {
+int ttcb_test_bounded_wait(uint64_t limit_ns, int arrive, unsigned int* gave_up) {
+  unsigned int* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned int));
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemset(d, 0, sizeof(unsigned int));
+  if (e == cudaSuccess) {
+    bounded_wait_kernel<<<1, 64>>>(limit_ns, arrive, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(gave_up, d, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return (int)e;
+}
+
+ttcb_status ttcb_plan_wait_timeouts(const ttcb_plan* p, unsigned int* count) {
+  if (!p || !count) return fail(TTCB_ERR_INVALID_ARG, "plan and count must not be NULL");
+  *count = 0;
+  if (!p->wait_status) return TTCB_OK;
+  cudaError_t e = cudaMemcpy(count, p->wait_status, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy of the wait status");
+  if (*count && (e = cudaMemset(p->wait_status, 0, sizeof(unsigned int))) != cudaSuccess)
+    return cuda_fail(e, "cudaMemset of the wait status");
+  return TTCB_OK;
 }
 
 int64_t ttcb_plan_bytes(const ttcb_plan* p) {

@@ -80,7 +80,10 @@ struct TileDesc {
   int32_t shiftA;     // 1: A runs are copied as covering 16-byte chunks (the vector width is V)
   int32_t shiftW;     // staged stride of one A run (elements, a multiple of V)
   int32_t shiftCM;    // chunk slots per A run
-  int32_t shift_pad_;
+  // 1: the staged kernel may move each A run with one bulk copy (cp.async.bulk, completion counted
+  // on a per-stage mbarrier) instead of per-thread 16-byte copies. The staged layout keeps every run
+  // contiguous and 16-byte aligned: sigmaA is a multiple of LA (or the runs are shifted).
+  int32_t bulkA;
   FastDiv divCM;      // divisor shiftCM
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
 };
@@ -103,3 +106,10 @@ enum { TTCB_KERNEL_TILE = 1, TTCB_KERNEL_ROW = 2 };
 // form with the fixed round-robin tile order or with tiles claimed in order from a counter (_DYN).
 enum { TTCB_KERNEL_TILE_FAST = 3, TTCB_KERNEL_TILE_ASYNC = 4, TTCB_KERNEL_TILE_ASYNC_REG = 5, TTCB_KERNEL_TILE_RAGGED = 6,
        TTCB_KERNEL_TILE_ASYNC_DYN = 7, TTCB_KERNEL_TILE_ASYNC_REG_DYN = 8 };
+// Added to a staged-kernel id: the form that moves A runs with bulk copies (TileDesc::bulkA).
+enum { TTCB_KERNEL_BULK_FLAG = 16 };
+inline bool ttcb_is_staged_kernel(int k) {
+  k &= ~TTCB_KERNEL_BULK_FLAG;
+  return k == TTCB_KERNEL_TILE_ASYNC || k == TTCB_KERNEL_TILE_ASYNC_REG || k == TTCB_KERNEL_TILE_ASYNC_DYN ||
+         k == TTCB_KERNEL_TILE_ASYNC_REG_DYN;
+}

@@ -452,6 +452,56 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Bulk copies global -> shared (cp.async.bulk): one instruction moves a contiguous, 16-byte aligned
+// range whose size is a multiple of 16 bytes, and signals the bytes it wrote to an mbarrier in
+// shared memory (complete_tx). A phase of the barrier completes once its one expected arrival has
+// come (arrive.expect_tx, which also adds the bytes to wait for) and every byte has landed.
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+// makes the initialised barriers visible to the bulk-copy unit before any copy signals them
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Waits for the barrier's phase of the given parity; false if it has not completed within limit_ns
+// (the copies it counts never landed). try_wait itself suspends the thread for a while between
+// checks, so the loop polls the clock only every 64 attempts.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t n = 1; n != 0; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((n & 63u) == 0 && global_ns() - t0 > limit_ns) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// A stage's bulk copies land within microseconds; a wait that lasts seconds means they never will.
+constexpr uint64_t kBulkWaitLimitNs = 2000000000ull;
+constexpr uint64_t kBulkDrainLimitNs = 200000000ull;  // the wait for the other stages, after that
+
 // Shared-memory layout of the staged kernel: S stages of [A tile (staged A order)][B tile (B order,
 // only when beta != 0)], then segA, segB, and gtab when the gather positions do not fit registers.
 constexpr int kRegPos = 16;  // gather positions per thread kept in registers (P <= kRegPos * kThreads)
@@ -510,7 +560,7 @@ constexpr int kInfoRing = 2 * kDecodeBatch;  // decoded-tile ring entries (tile 
 constexpr int kMaxStages = 7;                // S - 2 = D tiles in flight, D < kDecodeBatch
 static_assert(kMaxStages - 2 < kDecodeBatch && kMaxStages - 2 <= 5,
               "tiles in flight must be decoded a batch ahead and covered by the copy-group wait");
-constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileInfo);
+constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileInfo) + kMaxStages * sizeof(uint64_t);
 
 // REG: every tile-relative offset of this thread lives in registers (tiles of at most kRegVec
 // vectors per thread and side whose offsets fit 32 bits and whose staged bytes fit 16 bits): A
@@ -527,14 +577,21 @@ constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileIn
 // launch that uses them, which runs after this grid completes (stream order, and griddepcontrol.wait
 // before the first claim when the launch overlaps its predecessor).
 // a0 (shifted A runs only): A's pointer is a0 elements past a 16-byte boundary.
-template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN>
+// BULK (descriptor's bulkA; VA is the 16-byte vector): the lanes of warp 0 move each A run of a
+// tile with one bulk copy, and the stage's mbarrier counts the bytes; every thread waits on it before
+// the store phase, with a time limit. A wait that runs out adds 1 to *wait_status, waits (bounded
+// again) for the copies of the other tiles in flight and ends the CTA's loop, so that the host
+// learns of it and the context stays usable.
+template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN, bool BULK>
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
     tile_async_kernel(
     const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta,
-    unsigned int* __restrict__ sched, int a0) {
+    unsigned int* __restrict__ sched, int a0, unsigned int* __restrict__ wait_status) {
+  static_assert(!BULK || VA * sizeof(TA) == 16, "bulk copies move runs of whole 16-byte vectors");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
-  __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both
+  __shared__ TileInfo info[kInfoRing];  // kAsyncStaticSmem counts both, and the stage barriers
+  __shared__ __align__(8) uint64_t abar[kMaxStages];  // BULK: one mbarrier per stage
   const int tid = threadIdx.x;
   pdl_allow_next();
   for (int i = tid; i < (int)(sizeof(TileDesc) / 4); i += kThreads)
@@ -553,8 +610,9 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   {
     const int64_t* gA = reinterpret_cast<const int64_t*>(base + d.off_segA);
     const int64_t* gB = reinterpret_cast<const int64_t*>(base + d.off_segB);
-    if (!REG) {
+    if (!REG || BULK)
       for (int i = tid; i < d.nsegA; i += kThreads) segA[i] = gA[i];
+    if (!REG) {
       for (int i = tid; i < d.nsegB; i += kThreads) segB[i] = gB[i];
       if (!reg_pos) {
         const uint32_t* gG = reinterpret_cast<const uint32_t*>(ggtab);
@@ -601,7 +659,9 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       const int i = tid + u * kThreads;
       rA[u] = rB[u] = 0;
       if (!(u & 1)) dA[u >> 1] = 0;
-      if (i < nvA && shift) {
+      if (BULK) {
+        // the A runs are moved by warp 0's bulk copies
+      } else if (i < nvA && shift) {
         // chunk c of run s: source V * (segA[s] / V + c) past the tile's aligned base, slot
         // s * shiftW + V * c; it covers run elements for lo <= x < hi
         const int s = (int)fdiv((uint32_t)i, d.divCM);
@@ -650,6 +710,61 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     const TB* Bt = B + ti.bB;
     const uint32_t sb = stage0 + (uint32_t)stage * sbytes;
     const uint32_t sbB = sb + a_bytes;
+    if constexpr (BULK) {
+      if (tid < 32) {
+        const uint32_t bar = smem_u32(&abar[stage]);
+        const int LA = d.LA, nsegA = d.nsegA;
+        if (shift) {
+          // run s, y = segA[s] mod V: its elements sit at x + y + j past the aligned chunk
+          // segA[s] - y, so chunks (x + y) / V .. (x + y + LA - 1) / V hold it, every one of them
+          // holding at least one run element
+          uint32_t bytes = 0;
+          for (int s = tid; s < nsegA; s += 32) {
+            const int xy = x + (int)(segA[s] & (VA - 1));
+            bytes += (uint32_t)((xy + LA - 1) / VA - xy / VA + 1) * 16u;
+          }
+          bytes = __reduce_add_sync(0xffffffffu, bytes);
+          if (tid == 0) mbar_arrive_expect_tx(bar, bytes);
+          __syncwarp();
+          for (int s = tid; s < nsegA; s += 32) {
+            const int y = (int)(segA[s] & (VA - 1));
+            const int clo = (x + y) / VA, chi = (x + y + LA - 1) / VA;
+            bulk_g2s(sb + (uint32_t)((s * d.shiftW + VA * clo) * (int)sizeof(TA)), At + (segA[s] - y + VA * clo),
+                     (uint32_t)(chi - clo + 1) * 16u, bar);
+          }
+        } else {
+          // run s at its staged position s * LA + (s * LA / sigmaA) * padA, contiguous
+          if (tid == 0) mbar_arrive_expect_tx(bar, (uint32_t)(P * (int)sizeof(TA)));
+          __syncwarp();
+          const FastDiv divSig = d.divSigmaA;
+          const int padA = d.padA;
+          const uint32_t run_bytes = (uint32_t)(LA * (int)sizeof(TA));
+          for (int s = tid; s < nsegA; s += 32) {
+            const int p = s * LA;
+            const int sp = (int)fdiv((uint32_t)p, divSig);
+            bulk_g2s(sb + (uint32_t)((p + sp * padA) * (int)sizeof(TA)), At + segA[s], run_bytes, bar);
+          }
+        }
+      }
+      if constexpr (BETA) {
+        if constexpr (REG) {
+#pragma unroll
+          for (int u = 0; u < kRegVec; ++u) {
+            const int i = tid + u * kThreads;
+            if (i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
+          }
+        } else {
+          const int LB = d.LB;
+          const FastDiv divLB = d.divLB;
+          for (int i = tid; i < nvB; i += kThreads) {
+            const int q = i * VB;
+            const int s = (int)fdiv((uint32_t)q, divLB);
+            cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(q * sizeof(TB)), Bt + (segB[s] + (q - s * LB)));
+          }
+        }
+      }
+      return;
+    }
     if constexpr (REG) {
 #pragma unroll
       for (int u = 0; u < kRegVec; ++u) {
@@ -718,6 +833,13 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   // decoded in batches (see TileInfo).
   const int D = S - 2;
   unsigned int pending = 0;  // DYN: thread 0's claim for the tile of iteration k + D + 3
+  uint32_t phase = 0;        // BULK: bit s = parity of the next phase of stage s's barrier
+  if constexpr (BULK) {
+    if (tid == 0) {
+      for (int st = 0; st < S; ++st) mbar_init(smem_u32(&abar[st]), 1);
+      mbar_fence_init();
+    }
+  }
   if constexpr (DYN) {
     // claims touch no tensor data, but the previous launch's reset of the counter must be visible
     pdl_wait_previous();
@@ -750,16 +872,37 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       if (t >= ntiles) break;
     }
     issue(info[(k + D) % kInfoRing], nxt);
-    cp_async_commit();
-    // tile k's copies are complete once at most D groups (tiles k + 1 .. k + D) are pending
-    switch (D) {
-      case 1: cp_async_wait<1>(); break;
-      case 2: cp_async_wait<2>(); break;
-      case 3: cp_async_wait<3>(); break;
-      case 4: cp_async_wait<4>(); break;
-      default: cp_async_wait<5>(); break;
+    if (!BULK || BETA) {
+      cp_async_commit();
+      // tile k's copies are complete once at most D groups (tiles k + 1 .. k + D) are pending
+      switch (D) {
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        case 3: cp_async_wait<3>(); break;
+        case 4: cp_async_wait<4>(); break;
+        default: cp_async_wait<5>(); break;
+      }
     }
-    __syncthreads();
+    if constexpr (BULK) {
+      bool late = false;
+      if (info[k % kInfoRing].state == 1) {
+        late = !mbar_wait_bounded(smem_u32(&abar[cur]), (phase >> cur) & 1u, kBulkWaitLimitNs);
+        phase ^= 1u << cur;
+      }
+      if (__syncthreads_or(late)) {
+        // tile k's copies never landed: record it, wait (bounded) for the copies of tiles k .. k + D
+        // so that none writes shared memory after the CTA ends, and stop
+        if (tid == 0 && wait_status) atomicAdd(wait_status, 1u);
+        for (int j = 0, st = cur; j <= D; ++j, st = st + 1 == S ? 0 : st + 1) {
+          if (info[(k + j) % kInfoRing].state != 1) continue;
+          const uint32_t par = ((phase >> st) & 1u) ^ (j == 0 ? 1u : 0u);
+          mbar_wait_bounded(smem_u32(&abar[st]), par, kBulkDrainLimitNs);
+        }
+        break;
+      }
+    } else {
+      __syncthreads();
+    }
     if constexpr (DYN) {
       // the tile of iteration k + D + 2 (read after the next barrier), and the next claim, whose
       // result thread 0 needs only an iteration later (decoding here, before thread 0's own stores,

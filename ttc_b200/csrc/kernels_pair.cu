@@ -53,7 +53,7 @@ using TB = float2;
 #define PAIR_BATCH_FN pick_batch_zc
 #endif
 
-template <int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN>
+template <int VA, int VB, bool BETA, bool STREAM, bool REG, bool DYN, bool BULK>
 static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, const void* alpha, const void* beta,
                                 cudaStream_t stream, int blocks) {
   TA al;
@@ -80,41 +80,47 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   cfg.numAttrs = 1;
   // shifted A runs: A's pointer lies a0 elements past a 16-byte boundary
   const int a0 = (int)(((uintptr_t)A / sizeof(TA)) & (uintptr_t)(VA - 1));
-  return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG, DYN>,
+  return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG, DYN, BULK>,
                             reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A),
-                            static_cast<TB*>(B), al, be, sched, a0);
+                            static_cast<TB*>(B), al, be, sched, a0, BULK ? p->wait_status : nullptr);
 }
 
-template <int VA, int VB, bool REG, bool DYN>
+template <int VA, int VB, bool REG, bool DYN, bool BULK>
 static KernelRef async_ref(int variant) {
   KernelRef r;
   if (variant == 2) {
-    r.fn = &launch_async<VA, VB, true, false, REG, DYN>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, REG, DYN>);
+    r.fn = &launch_async<VA, VB, true, false, REG, DYN, BULK>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, true, false, REG, DYN, BULK>);
   } else if (variant == 1) {
-    r.fn = &launch_async<VA, VB, false, true, REG, DYN>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, REG, DYN>);
+    r.fn = &launch_async<VA, VB, false, true, REG, DYN, BULK>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, true, REG, DYN, BULK>);
   } else {
-    r.fn = &launch_async<VA, VB, false, false, REG, DYN>;
-    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, REG, DYN>);
+    r.fn = &launch_async<VA, VB, false, false, REG, DYN, BULK>;
+    r.func = reinterpret_cast<const void*>(&tile_async_kernel<TA, TB, VA, VB, false, false, REG, DYN, BULK>);
   }
   return r;
 }
 
-template <int VA, bool REG, bool DYN>
+template <int VA, bool REG, bool DYN, bool BULK>
 static KernelRef async_ref_b(int vb, int variant) {
   constexpr int MB = 16 / sizeof(TB);
-  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), REG, DYN>(variant);
-  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), REG, DYN>(variant);
-  return async_ref<VA, 1, REG, DYN>(variant);
+  if (vb >= 4 && MB >= 4) return async_ref<VA, (MB >= 4 ? 4 : 1), REG, DYN, BULK>(variant);
+  if (vb >= 2 && MB >= 2) return async_ref<VA, (MB >= 2 ? 2 : 1), REG, DYN, BULK>(variant);
+  return async_ref<VA, 1, REG, DYN, BULK>(variant);
 }
 
-template <bool REG, bool DYN>
+// The bulk-copy form exists for the full 16-byte A vector only (the launch asks for it only then).
+template <bool REG, bool DYN, bool BULK>
 static KernelRef async_ref_ab(int va, int vb, int variant) {
   constexpr int MA = 16 / sizeof(TA);
-  if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), REG, DYN>(vb, variant);
-  if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), REG, DYN>(vb, variant);
-  return async_ref_b<1, REG, DYN>(vb, variant);
+  if constexpr (BULK) {
+    if (va != MA) return KernelRef{};
+    return async_ref_b<MA, REG, DYN, true>(vb, variant);
+  } else {
+    if (va >= 4 && MA >= 4) return async_ref_b<(MA >= 4 ? 4 : 1), REG, DYN, false>(vb, variant);
+    if (va >= 2 && MA >= 2) return async_ref_b<(MA >= 2 ? 2 : 1), REG, DYN, false>(vb, variant);
+    return async_ref_b<1, REG, DYN, false>(vb, variant);
+  }
 }
 
 template <int VA, int VB, bool BETA, bool STREAM, bool FAST>
@@ -238,10 +244,15 @@ KernelRef PAIR_FN(int kernel, int va, int vb, int variant) {
     return row_ref<1>(variant);
   }
   if (kernel == TTCB_KERNEL_TILE_FAST) return tile_ref_ab<true>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false, false>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true, false>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC_DYN) return async_ref_ab<false, true>(va, vb, variant);
-  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG_DYN) return async_ref_ab<true, true>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC) return async_ref_ab<false, false, false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG) return async_ref_ab<true, false, false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_DYN) return async_ref_ab<false, true, false>(va, vb, variant);
+  if (kernel == TTCB_KERNEL_TILE_ASYNC_REG_DYN) return async_ref_ab<true, true, false>(va, vb, variant);
+  if (kernel == (TTCB_KERNEL_TILE_ASYNC | TTCB_KERNEL_BULK_FLAG)) return async_ref_ab<false, false, true>(va, vb, variant);
+  if (kernel == (TTCB_KERNEL_TILE_ASYNC_REG | TTCB_KERNEL_BULK_FLAG)) return async_ref_ab<true, false, true>(va, vb, variant);
+  if (kernel == (TTCB_KERNEL_TILE_ASYNC_DYN | TTCB_KERNEL_BULK_FLAG)) return async_ref_ab<false, true, true>(va, vb, variant);
+  if (kernel == (TTCB_KERNEL_TILE_ASYNC_REG_DYN | TTCB_KERNEL_BULK_FLAG))
+    return async_ref_ab<true, true, true>(va, vb, variant);
   if (kernel == TTCB_KERNEL_TILE_RAGGED) return ragged_ref(variant);
   return tile_ref_ab<false>(va, vb, variant);
 }

@@ -455,8 +455,9 @@ static constexpr double kTargetInFlightBytes = 18.0 * 1024 * 1024;
 // GPU span W = c * SMs * (S - 1) * tile bytes of A and B. The planner keeps every CTA an SM holds
 // (c = 0: timed over the whole 64-case 200 MiB sweep back to back, fewer CTAs per SM lost 2% with
 // three and 12% with two, although single cases repeated alone ran faster with them) and picks the
-// S in 3..6 whose W comes nearest 18 MiB: with S fixed at 3 or 4 for every case the sweep measured
-// within 0.5% of this rule, and for single cases rings far from it lost 5-15%. Problems too small to
+// S in 3..6 whose W comes nearest 18 MiB, among the rings that let two CTAs share an SM when there
+// are any: with S fixed at 3 or 4 for every case the sweep measured within 0.5% of the W rule, and for
+// single cases rings far from it lost 5-15%. Problems too small to
 // fill the GPU twice keep the earlier rule (four stages while four CTAs fit, else three).
 // smem_for(S) is the dynamic shared memory of an S-stage ring; fixed_S (3..kMaxStages, else 0) is a
 // schedule's explicit ring depth.
@@ -473,8 +474,11 @@ static StageChoice choose_stages(int64_t P, int EA, int EB, bool beta, int vecA,
   const bool fixed = fixed_S >= 3 && fixed_S <= ttcb::kMaxStages;
   const int64_t tile_bytes = P * (int64_t)(EA + EB * (beta ? 2 : 1));
   const int reg_ctas = ttcb::async_min_blocks(vecA * EA, vecB * EB, beta);
+  // rings that leave room for a second CTA on each SM come first: with one CTA per SM the SM idles
+  // at every tile barrier (the 1000x768x16 fp32 beta = 1 transposition ran at 4.4 TB/s with four
+  // stages and one CTA per SM, at 5.4 TB/s with three stages and two)
   double best = 1e30;
-  int bS = 0;
+  int bS = 0, bc = 0;
   for (int S = 3; S <= 6; ++S) {
     if (fixed && S != fixed_S) continue;
     if (smem_for(S) > 200 * 1024) continue;
@@ -483,9 +487,12 @@ static StageChoice choose_stages(int64_t P, int EA, int EB, bool beta, int vecA,
     if (cmax < 1) continue;
     const double W = (double)cmax * kPlanSMs * (S - 1) * (double)tile_bytes;
     const double key = std::fabs(std::log(W / kTargetInFlightBytes));
-    if (key < best - 1e-9) {
+    const bool better = bS == 0 || (std::min(cmax, 2) > std::min(bc, 2)) ||
+                        (std::min(cmax, 2) == std::min(bc, 2) && key < best - 1e-9);
+    if (better) {
       best = key;
       bS = S;
+      bc = cmax;
     }
   }
   if (bS && nfull >= 2LL * 4 * kPlanSMs) out.S = bS;
@@ -501,6 +508,13 @@ static bool wants_shifted_runs(const TileCand& c, int EA, const ttcb_tuning& tu)
   const int VM = 16 / EA;
   return EA < 16 && c.vecA < VM && c.LA >= 2 * VM && tu.vec != 1 && tu.shifted_runs == 1 &&
          (tu.tile_variant == 0 || tu.tile_variant == 3);
+}
+
+// Bulk A copies (TileDesc::bulkA) when the schedule asks for them and each A run can be one
+// 16-byte aligned bulk copy: 16-byte vectors reach every run, or the runs are shifted.
+static bool wants_bulk_copies(const TileCand& c, int EA, const ttcb_tuning& tu, bool shift) {
+  return tu.bulk_copies == 1 && tu.vec != 1 && (tu.tile_variant == 0 || tu.tile_variant == 3) &&
+         (shift || c.vecA * EA == 16);
 }
 
 static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
@@ -566,6 +580,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   // (fp32) or LA / 2 (fp64) narrow ones. Run s then sits at s * shiftW + (segA[s] mod V).
   const int VM = 16 / EA;
   const bool shift = wants_shifted_runs(c, EA, p->tuning);
+  // bulk copies keep each run contiguous: the padding period is then a multiple of the run
+  const bool bulk = wants_bulk_copies(c, EA, p->tuning, shift);
   const int64_t CM = shift ? (2 * VM - 3 + c.LA) / VM + 1 : 0;  // chunk slots per run
   int64_t shiftW = CM * VM;
   auto staged_shift = [&](int64_t pp, int64_t W) {
@@ -631,6 +647,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     }
     for (int64_t sg : sigmas) {
       if (shift || best_cost == ideal) break;
+      if (bulk && sg % c.LA != 0) continue;
       sigma = sg;
       for (int k = 0; k <= 8; ++k) {
         const int64_t cand = (int64_t)k * c.vecA;
@@ -667,6 +684,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   td.shiftA = shift ? 1 : 0;
   td.shiftW = (int32_t)(shift ? shiftW : 0);
   td.shiftCM = (int32_t)CM;
+  td.bulkA = bulk ? 1 : 0;
   td.divCM = make_fastdiv((uint32_t)std::max<int64_t>(CM, 1));
   td.P = (int32_t)P;
   td.LA = (int32_t)c.LA;
@@ -793,8 +811,9 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
                    smem_for(td.nstages) <= 200 * 1024) ? 1 : 0;
     p->smem_async = (int)smem_for(td.nstages);
     td.reg_ok = (td.fast && td.stage_elems * (int64_t)EA < 65536 && P * (int64_t)EB < 65536) ? 1 : 0;
-    // with shifted runs every chunk slot is a copy: the register path holds four per thread
-    if (shift && (P / c.LA) * CM > 4 * 256) td.reg_ok = 0;
+    // with shifted runs every chunk slot is a copy: the register path holds four per thread (bulk
+    // copies of shifted runs hold none)
+    if (shift && !bulk && (P / c.LA) * CM > 4 * 256) td.reg_ok = 0;
     // the staged kernel leaves ragged tiles to the ragged-tile kernel, whose tables must fit too
     if (td.nrag0 + td.nrag1 > 0 && ttcb::ragged_smem_bytes((int)phys_size, EA, (int)P) > 200 * 1024) td.async_ok = 0;
   }
@@ -1037,6 +1056,7 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   if (p->shape_only) {
     p->vecA = wants_shifted_runs(best, EA, p->tuning) ? 16 / EA : best.vecA;
     p->shape_shifted = wants_shifted_runs(best, EA, p->tuning);
+    p->shape_bulk = wants_bulk_copies(best, EA, p->tuning, p->shape_shifted);
     p->vecB = best.vecB;
     p->est_cost = best.cost;
     // the staged kernel's ring depth and CTAs per SM, from the staged layout's usual size (the bank
@@ -1153,7 +1173,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
       << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
       << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm
-      << ",\"shifted_runs\":" << t->shiftA << ",\"claims\":" << (p->claim_words ? 1 : 0)
+      << ",\"shifted_runs\":" << t->shiftA << ",\"bulk\":" << t->bulkA << ",\"claims\":" << (p->claim_words ? 1 : 0)
       << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
@@ -1162,6 +1182,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
     o << ",\"tile\":{\"P\":" << p->tile_P << ",\"LA\":" << p->tile_LA << ",\"LB\":" << p->tile_LB
       << ",\"ntiles\":" << p->tile_ntiles << ",\"fast\":" << (fits ? 1 : 0) << ",\"stages\":" << p->shape_stages
       << ",\"ctas_per_sm\":" << p->ctas_per_sm << ",\"shifted_runs\":" << (p->shape_shifted ? 1 : 0)
+      << ",\"bulk\":" << (p->shape_bulk ? 1 : 0)
       << ",\"shape_only\":1,\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";

@@ -76,6 +76,9 @@ struct ttcb_plan {
   // creation, reset by each launch's last CTA) and the host's running launch count
   unsigned int* claim_words = nullptr;
   void* launch_count = nullptr;  // std::atomic<unsigned int>
+  // staged kernel with bulk A copies: count of stage waits that ran out of time (device word, zeroed
+  // at creation; read and cleared by ttcb_plan_wait_timeouts)
+  unsigned int* wait_status = nullptr;
   int smem_ragged = 0;    // its dynamic shared memory (two tile buffers + tables)
   int device = 0;
 
@@ -96,6 +99,7 @@ struct ttcb_plan {
   int64_t tile_ext[TTCB_MAXR] = {0};  // tile extent per fused dimension (0 = not in the tile)
   int shape_stages = 0;                // the staged kernel's ring depth the schedule would use
   bool shape_shifted = false;          // the staged kernel would copy shifted A runs
+  bool shape_bulk = false;             // the staged kernel would move A runs with bulk copies
 };
 
 // Fills everything except dev_desc / blocks (which need the CUDA device). Returns a status and a

@@ -1,5 +1,5 @@
-// Test hooks exported by libttcb200.so for CPU-side unit tests. They are not part of the public
-// ABI (include/ttcb200.h) and make no CUDA calls.
+// Test hooks exported by libttcb200.so for unit tests. They are not part of the public ABI
+// (include/ttcb200.h); all but ttcb_test_bounded_wait make no CUDA calls.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -23,11 +23,16 @@ void ttcb_test_desc_layout(int64_t* out);
 size_t ttcb_test_plan_shapes(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
                              int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tunings, int n, char* buf,
                              size_t len);
-// The boxes a plan's ragged tiles are moved as (edge plans), host-only: a JSON array of
-// {"rank","perm","size","lda","ldb","offA","offB"}; returns the length needed, 0 on failure.
 // Lowers the largest descriptor ttcb_transpose_noalloc accepts to `bytes` (0 restores the full
 // scratch size) and returns the scratch size. Makes no CUDA call.
 size_t ttcb_test_noalloc_limit(size_t bytes);
+// The boxes a plan's ragged tiles are moved as (edge plans), host-only: a JSON array of
+// {"rank","perm","size","lda","ldb","offA","offB"}; returns the length needed, 0 on failure.
 size_t ttcb_test_plan_edges(int rank, const int* perm, const int64_t* size, const int64_t* lda, const int64_t* ldb,
                             int type_a, int type_b, int beta_nonzero, const ttcb_tuning* tuning, char* buf, size_t len);
+// GPU hook (the one that launches a kernel): one CTA waits, with a limit of limit_ns, on an mbarrier
+// phase - the bounded wait of the staged kernel's bulk-copy form. With arrive = 0 nothing completes
+// the phase, so the wait must give up; with arrive = 1 the CTA arrives first, so it must not. Writes
+// to *gave_up how many CTAs gave up (0 or 1); returns the CUDA error code.
+int ttcb_test_bounded_wait(uint64_t limit_ns, int arrive, unsigned int* gave_up);
 }

@@ -113,7 +113,7 @@ def emit_shim(ttcArgs, file_name: str, func: str, tuning: dict, size, perm, lda,
     from ._native import Tuning
     packed = Tuning.make(**tuning)  # an explicit loop order travels as raster_lo/raster_hi
     fields = " ".join(f"t.{k} = {int(getattr(packed, k))};" for k, _ in Tuning._fields_
-                      if k != "reserved" and int(getattr(packed, k)) != 0)
+                      if int(getattr(packed, k)) != 0)
     a_val = f"{SCALAR[ta]} a[2] = {{alpha, 0}};" if "complex" in ta else f"{SCALAR[ta]} a[1] = {{alpha}};"
     b_val = (f"{SCALAR[tb]} b[2] = {{beta, 0}};" if "complex" in tb else f"{SCALAR[tb]} b[1] = {{beta}};") \
         if beta else f"{SCALAR[tb]}* b = 0;"
