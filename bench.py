@@ -67,8 +67,8 @@ def parse(argv=None):
                          "batched workload with the planner's schedules launched --reps times (for profilers)")
     ap.add_argument("--schedule", default="learned", choices=["default", "learned"],
                     help="sweep: the planner's default schedule per case, or the learned selector's choice "
-                         "(chosen before the timed region: its top-1, timed against the planner default when "
-                         "its confidence is low)")
+                         "(chosen before the timed region: its top-1 on a large predicted gain over the "
+                         "planner default, the faster of the two, timed, on a moderate one)")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
     ap.add_argument("--reps", type=int, default=3, help="case / batchcase: launches")
     ap.add_argument("--tuning", default=None, help="case: a schedule (JSON of ttcb_tuning fields) instead of the "

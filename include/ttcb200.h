@@ -84,16 +84,17 @@ typedef struct {
                             copies in flight); 0 = planner's choice                             */
   int32_t ctas_per_sm;   /* staged tile kernel: resident CTAs per SM (1..8, capped by what fits);
                             0 = planner's choice. `blocks`, when set, takes precedence          */
-  int32_t round_robin;   /* staged tile kernel: 0 = planner's choice (the round-robin order),
-                            1 = fixed round-robin order (tile blockIdx + k * CTAs), -1 = CTAs
-                            claim tiles in order from counters the plan owns                    */
+  int32_t round_robin;   /* staged tile kernel: 0 = planner's choice (claims for tiles of 16 KiB
+                            or more when every CTA has 16 or more), 1 = fixed round-robin order
+                            (tile blockIdx + k * CTAs), -1 = CTAs claim tiles in order from
+                            counters the plan owns                                              */
   int32_t shifted_runs;  /* staged tile kernel: 1 = copy A runs that 16-byte accesses cannot
                             reach directly (odd lengths or offsets) as the 16-byte chunks that
                             cover them; 0 = planner's choice (plain copies), -1 = never         */
-  int32_t bulk_copies;   /* staged tile kernel: 1 = move each A run with one bulk copy
-                            (cp.async.bulk into the stage, completion counted on an mbarrier)
-                            where the runs allow it (16-byte aligned runs, or shifted runs);
-                            0 = planner's choice (per-thread 16-byte copies), -1 = never       */
+  int32_t bulk_copies;   /* staged tile kernel: 1 = move A with one bulk copy per run or run
+                            piece (cp.async.bulk into the stage, completion counted on an
+                            mbarrier) where the runs allow it (16-byte aligned runs, or shifted
+                            runs); 0 or -1 = per-thread 16-byte copies                          */
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;
@@ -117,10 +118,10 @@ ttcb_status ttcb_plan_create(ttcb_plan** plan, int rank, const int* perm, const 
  * plan created with beta_nonzero == 0. */
 ttcb_status ttcb_transpose(const ttcb_plan* plan, const void* A, void* B, const void* alpha,
                            const void* beta, ttcb_stream_t stream);
-/* Calls with one plan may overlap on the GPU (several streams). A plan whose schedule claims tiles
- * from counters (round_robin = -1) takes the counter words in turn from 64 slot pairs, so up to 64
- * of its launches can be in flight at once; a launch captured in a CUDA graph keeps its slot, and
- * replays of that graph must not overlap each other. */
+/* Calls with one plan may overlap on the GPU (several streams). A plan whose staged kernel claims
+ * tiles from counters ("claims" in its description) takes the counter words in turn from 64 slot
+ * pairs, so up to 64 of its launches can be in flight at once; a launch captured in a CUDA graph
+ * keeps its slot, and replays of that graph must not overlap each other. */
 
 /* Allocation-free transposition, for callers that may not allocate device memory (their memory is
  * owned by an external pool, or cudaMalloc is forbidden where they run). It has no counterpart in

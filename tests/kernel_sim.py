@@ -108,6 +108,8 @@ def parse_tile(b):
     t["gtab"] = np.frombuffer(b, dtype=np.uint16, count=t["P"], offset=t["off_gtab"]).astype(np.int64)
     o = L["off_shiftA"]
     t["shiftA"], t["shiftW"], t["shiftCM"], t["bulkA"] = _i32(b, o), _i32(b, o + 4), _i32(b, o + 8), _i32(b, o + 12)
+    t["bulk_pieces"] = _i32(b, o + 16 + L["fastdiv_size"])
+    t["divPieces"] = _fd(b, o + 32 + L["fastdiv_size"])
     return t
 
 
@@ -129,18 +131,27 @@ def check_bulk_layout(t, EA):
     want = segA[p_of_q // LA] + p_of_q % LA
     stage_bytes = ((t["stage_elems"] * EA + 15) // 16) * 16
     if not t["shiftA"]:
-        assert t["sigmaA"] % LA == 0, "a padding point splits a run"
-        assert (LA * EA) % 16 == 0 and (segA * EA % 16 == 0).all()
+        m = t["bulk_pieces"]
+        assert m >= 1 and LA % m == 0
+        piece = LA // m
+        if m == 1:
+            assert t["sigmaA"] % LA == 0, "a padding point splits a run"
+        else:
+            assert t["sigmaA"] == piece, "pieces are not cut at the padding points"
+        assert (piece * EA) % 16 == 0 and (segA * EA % 16 == 0).all()
         for g in t["g"]:
             assert (g["strideA"] * EA) % 16 == 0, "a tile base off the 16-byte grid"
         src = np.full(stage_bytes // EA + V, -(1 << 60), np.int64)
         total = 0
-        for s in range(nseg):
-            p = s * LA
+        for i in range(nseg * m):
+            s = int(fdiv(i, t["divPieces"]))
+            j = i - s * m
+            assert s == i // m
+            p = s * LA + j * piece
             dst = p + (p // t["sigmaA"]) * t["padA"]
-            assert (dst * EA) % 16 == 0 and (dst + LA) * EA <= stage_bytes
-            src[dst:dst + LA] = segA[s] + np.arange(LA)
-            total += LA * EA
+            assert (dst * EA) % 16 == 0 and (dst + piece) * EA <= stage_bytes
+            src[dst:dst + piece] = segA[s] + j * piece + np.arange(piece)
+            total += piece * EA
         assert total == P * EA
         assert np.array_equal(src[t["gtab"]], want), "a gather reads an element no bulk copy brought"
         return

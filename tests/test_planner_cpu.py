@@ -404,16 +404,20 @@ def test_shifted_a_runs_replay():
 
 
 def test_bulk_copy_layout_replay():
-    """Bulk A copies (tuning bulk_copies = 1, alone and with shifted runs): for random problems, the
-    CPU replay of warp 0's bulk copies (kernel_sim.check_bulk_layout) must keep every copy on 16-byte
-    boundaries and inside its stage and bring every element the store phase gathers; plans whose runs
-    allow no bulk copy must not ask for them; and the element mapping must equal the oracle's."""
+    """Bulk A copies (asked for by bulk_copies = 1, alone and with shifted runs, and the planner's own
+    choice): for random problems, the CPU replay of warp 0's bulk copies (kernel_sim.check_bulk_layout)
+    must keep every copy on 16-byte boundaries and inside its stage, cut runs into pieces only at the
+    padding points, and bring every element the store phase gathers; plans whose runs allow no bulk
+    copy must not ask for them; and the element mapping must equal the oracle's."""
     rng = np.random.default_rng(12)
     seen = {0: 0, 1: 0}
+    pieces = 0
     for it in range(70):
-        perm, size, lda, ldb = _random_problem(rng, max_rank=4, max_ext=24)
+        # every other problem rank 2 with long extents (long runs, cut into pieces)
+        perm, size, lda, ldb = _random_problem(rng, max_rank=4, max_ext=24) if it % 2 else \
+            _random_problem(rng, max_rank=2, max_ext=600)
         for dtype in ("s", "d", "c", "z", "sd"):
-            for tu in ({"bulk_copies": 1}, {"bulk_copies": 1, "shifted_runs": 1}):
+            for tu in ({"bulk_copies": 1}, {"bulk_copies": 1, "shifted_runs": 1}, None):
                 try:
                     kind, b = kernel_sim.host_desc(perm, size, dtype, False, lda, ldb, tu)
                 except TTCError:
@@ -424,12 +428,13 @@ def test_bulk_copy_layout_replay():
                 j = plan_host_json(perm, size, dtype, False, lda, ldb, tu)
                 EA = {"s": 4, "d": 8, "c": 8, "z": 16}[dtype[0]]
                 if not t["bulkA"]:
-                    assert not t["shiftA"] and j["vecA"] * EA != 16
+                    assert tu is None or (not t["shiftA"] and j["vecA"] * EA != 16)
                     continue
                 seen[t["shiftA"]] += 1
+                pieces += int(t["bulk_pieces"] > 1)
                 kernel_sim.check_bulk_layout(t, EA)
                 kernel_sim.check_staged_layout(t, j["vecA"])
                 _, (a, bb) = kernel_sim.simulate(perm, size, dtype, False, lda, ldb, tu)
                 wa, wb = _oracle_pairs(perm, size, lda, ldb)
                 assert dict(zip(bb.tolist(), a.tolist())) == dict(zip(wb.tolist(), wa.tolist()))
-    assert seen[0] >= 40 and seen[1] >= 20, seen
+    assert seen[0] >= 40 and seen[1] >= 20 and pieces >= 5, (seen, pieces)

@@ -132,7 +132,9 @@ def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
             W = c * SMS * (S - 1) * tile_bytes
             # fewer CTAs than fit cost the sweep 2-12%, so they come after every full-occupancy ring
             opts.append((c != cmax(S), abs(math.log(W / TARGET_IN_FLIGHT)), c, S))
-    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]] + [{"round_robin": -1}]
+    out = [{"stages": S, "ctas_per_sm": c} for _, _, c, S in sorted(opts)[:k]]
+    # the other tile order and the other way of moving A than the planner's
+    out.append({"round_robin": 1 if staged_claims(p, {}, desc) else -1})
     vm = 16 // ea
     if desc.get("vecA", vm) * ea == 16:
         out.append({"bulk_copies": 1})
@@ -140,6 +142,28 @@ def schedule_alternatives(p: Problem, desc: dict, k: int) -> list[dict]:
         # A runs that 16-byte copies cannot reach directly, copied as covering 16-byte chunks
         out += [{"shifted_runs": 1}, {"shifted_runs": 1, "bulk_copies": 1}]
     return out
+
+
+def staged_claims(p: Problem, tuning: dict, desc: dict) -> bool:
+    """Whether the staged kernel claims tiles from counters under this schedule: asked for
+    (round_robin -1), or the planner's rule for round_robin 0 - tiles of 16 KiB or more (A, B and B
+    read back) with 16 or more per CTA (CTAs estimated as SMs x the schedule's CTAs per SM, else as
+    many as the ring's shared memory lets share an SM)."""
+    rr = tuning.get("round_robin", 0)
+    if rr != 0:
+        return rr == -1
+    t = desc.get("tile") or {}
+    if desc.get("kernel") != "tile" or not t.get("P"):
+        return False
+    ta, tb = split_dtype(p.dtype)
+    tile_bytes = t["P"] * (ELEM_BYTES[ta] + ELEM_BYTES[tb] * (2 if p.beta_nonzero else 1))
+    c = tuning.get("ctas_per_sm") or t.get("ctas_per_sm") or 0
+    if not c:
+        stage = t["P"] * ELEM_BYTES[ta] * 1.07 + (t["P"] * ELEM_BYTES[tb] if p.beta_nonzero else 0)
+        S = tuning.get("stages") or t.get("stages") or 3
+        c = max(1, min(4, int(227 * 1024 // (S * stage + 3 * 1024))))
+    ctas = tuning.get("blocks") or c * SMS
+    return tile_bytes >= 16 * 1024 and t.get("ntiles", 0) >= 16 * ctas
 
 
 def fused_groups(p: Problem):

@@ -29,7 +29,7 @@ from typing import Optional
 import numpy as np
 
 from . import _native
-from .autotune import Problem, candidate_tunings, measure, Bench
+from .autotune import Problem, candidate_tunings, measure, Bench, staged_claims
 from .core import ELEM_BYTES, plan_shapes, split_dtype
 
 MAXD = 6
@@ -141,8 +141,7 @@ def candidate_features(p: Problem, tuning: dict, desc: dict, shape=None, groups=
     waves = nt / ctas
     f += [math.log2(max(waves, 1e-3)) / 10.0, waves - math.floor(waves)] + tail
     # how the staged kernel moves the tiles: claimed in order or round robin; A runs shifted; bulk copies
-    f += [1.0 if tuning.get("round_robin", 0) == -1 else 0.0, float(t.get("shifted_runs", 0)),
-          float(t.get("bulk", 0))]
+    f += [1.0 if staged_claims(p, tuning, desc) else 0.0, float(t.get("shifted_runs", 0)), float(t.get("bulk", 0))]
     f += _raster_jumps(p, tuning, desc, groups)
     return f
 

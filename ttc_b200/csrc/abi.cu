@@ -86,9 +86,12 @@ unsigned int* plan_claim_slot(const ttcb_plan* p) {
 using ttcb::allow_large_smem;
 using ttcb::needs_large_smem;
 
-// The staged kernel claims tiles from the plan's counters when the schedule asks for it
-// (round_robin = -1, and the plan then has counters); otherwise it takes the round-robin order.
+// The staged kernel claims tiles from the plan's counters when the plan has them (the schedule asks
+// for it with round_robin = -1, or the planner's rule below); otherwise it takes the round-robin
+// order.
 static bool uses_claims(const ttcb_plan* p) { return p->claim_words != nullptr; }
+static constexpr int64_t kClaimMinTileBytes = 16 * 1024;
+static constexpr int kClaimMinTilesPerCta = 16;
 // The staged kernel moves A runs with bulk copies when the plan's layout allows it and A's pointer
 // meets the layout's alignment (shifted runs take any pointer; plain runs need the 16-byte vector).
 static bool uses_bulk(const ttcb_plan* p, const TileDesc* td, int va, int EA) {
@@ -160,11 +163,20 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       if (s != TTCB_OK) return s;
     }
     if (td->async_ok) {
-      // Tiles are claimed in order from counters only when the schedule asks for it: timed over the
-      // 200 MiB sweep back to back the claims were 0.5-1% slower than the round-robin order and on
-      // the 147 MB 1000x768x16 transposition 15% slower; and a CTA claims its first S tiles at once,
-      // which on problems of a few tiles per CTA leaves most CTAs idle.
-      if (p->tuning.round_robin == -1) {
+      // Tiles are claimed in order from counters when the schedule asks for it, or by default for
+      // tiles of 16 KiB or more (A, B and B read back) when every CTA has at least 16 of them. Timed
+      // over the 200 MiB sweep back to back, claims made such tiles 2-15% faster (CTAs stay on
+      // neighbouring tiles, so the tiles in motion span a narrow stretch of A and B) and smaller
+      // ones up to 19% slower (the claim's round trip is not hidden behind a short tile); a CTA
+      // claims its first S tiles at once, which leaves CTAs idle when each has only a few (the 147 MB
+      // 1000x768x16 transposition, 11 tiles per CTA: 10% slower).
+      const int EA = dtype_bytes(p->ta);
+      s = grid_for(staged_kernel_id(p, td, td->reg_ok, false), p->smem_async, &p->blocks_async, td->nfull);
+      if (s != TTCB_OK) return s;
+      const int64_t tile_bytes = (int64_t)td->P * (EA + dtype_bytes(p->tb) * (p->beta_nonzero ? 2 : 1));
+      const bool claims_by_default = p->tuning.round_robin == 0 && tile_bytes >= kClaimMinTileBytes &&
+                                     td->nfull >= (int64_t)kClaimMinTilesPerCta * p->blocks_async;
+      if (p->tuning.round_robin == -1 || claims_by_default) {
         e = cudaMalloc(&p->claim_words, sizeof(unsigned int) * 2 * ttcb::kClaimSlots);
         if (e != cudaSuccess) {
           p->claim_words = nullptr;
@@ -186,7 +198,6 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
         if ((e = cudaMemset(p->wait_status, 0, sizeof(unsigned int))) != cudaSuccess)
           return cuda_fail(e, "cudaMemset of the wait status");
       }
-      const int EA = dtype_bytes(p->ta);
       s = grid_for(staged_kernel_id(p, td, td->reg_ok, uses_bulk(p, td, p->vecA, EA)), p->smem_async, &p->blocks_async,
                    td->nfull);
       if (s != TTCB_OK) return s;

@@ -80,11 +80,15 @@ struct TileDesc {
   int32_t shiftA;     // 1: A runs are copied as covering 16-byte chunks (the vector width is V)
   int32_t shiftW;     // staged stride of one A run (elements, a multiple of V)
   int32_t shiftCM;    // chunk slots per A run
-  // 1: the staged kernel may move each A run with one bulk copy (cp.async.bulk, completion counted
-  // on a per-stage mbarrier) instead of per-thread 16-byte copies. The staged layout keeps every run
-  // contiguous and 16-byte aligned: sigmaA is a multiple of LA (or the runs are shifted).
+  // 1: the staged kernel may move A with bulk copies (cp.async.bulk, completion counted on a
+  // per-stage mbarrier) instead of per-thread 16-byte copies: one per shifted run, else one per
+  // contiguous piece of a run in the staged layout - the whole run when sigmaA is a multiple of LA,
+  // else bulk_pieces = LA / sigmaA pieces of sigmaA elements, each 16-byte aligned.
   int32_t bulkA;
   FastDiv divCM;      // divisor shiftCM
+  int32_t bulk_pieces;  // bulk copies per A run (plain runs)
+  int32_t bulk_pad_[3];
+  FastDiv divPieces;  // divisor bulk_pieces
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
 };
 

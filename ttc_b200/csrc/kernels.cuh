@@ -733,16 +733,19 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
                      (uint32_t)(chi - clo + 1) * 16u, bar);
           }
         } else {
-          // run s at its staged position s * LA + (s * LA / sigmaA) * padA, contiguous
+          // piece j of run s (m = bulk_pieces pieces of LA / m elements, cut at the padding points)
+          // at its staged position p + (p / sigmaA) * padA, p = s * LA + j * LA / m, contiguous
           if (tid == 0) mbar_arrive_expect_tx(bar, (uint32_t)(P * (int)sizeof(TA)));
           __syncwarp();
-          const FastDiv divSig = d.divSigmaA;
-          const int padA = d.padA;
-          const uint32_t run_bytes = (uint32_t)(LA * (int)sizeof(TA));
-          for (int s = tid; s < nsegA; s += 32) {
-            const int p = s * LA;
+          const FastDiv divSig = d.divSigmaA, divM = d.divPieces;
+          const int padA = d.padA, m = d.bulk_pieces, piece = LA / m;
+          const uint32_t piece_bytes = (uint32_t)(piece * (int)sizeof(TA));
+          for (int i = tid; i < nsegA * m; i += 32) {
+            const int s = (int)fdiv((uint32_t)i, divM);
+            const int j = i - s * m;
+            const int p = s * LA + j * piece;
             const int sp = (int)fdiv((uint32_t)p, divSig);
-            bulk_g2s(sb + (uint32_t)((p + sp * padA) * (int)sizeof(TA)), At + segA[s], run_bytes, bar);
+            bulk_g2s(sb + (uint32_t)((p + sp * padA) * (int)sizeof(TA)), At + (segA[s] + j * piece), piece_bytes, bar);
           }
         }
       }

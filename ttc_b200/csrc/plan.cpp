@@ -510,9 +510,14 @@ static bool wants_shifted_runs(const TileCand& c, int EA, const ttcb_tuning& tu)
          (tu.tile_variant == 0 || tu.tile_variant == 3);
 }
 
-// Bulk A copies (TileDesc::bulkA) when the schedule asks for them and each A run can be one
-// 16-byte aligned bulk copy: 16-byte vectors reach every run, or the runs are shifted.
-static bool wants_bulk_copies(const TileCand& c, int EA, const ttcb_tuning& tu, bool shift) {
+// Bulk A copies (TileDesc::bulkA): possible on the staged kernel when 16-byte vectors reach every A
+// run, or the runs are shifted; used when the schedule asks for them (bulk_copies = 1). Timed over
+// the 200 MiB sweep back to back with round-robin tiles, copies of 320 bytes and more were up to 22%
+// faster than per-thread copies (mean +5%) and shorter ones 16-86% slower (a bulk copy costs the copy
+// unit about as much as a short run gains); with the planner's claimed tiles their effect ranged
+// from -21% to +11% per case with no rule in the run length, beta or tile size that separates the
+// two, and the sweep as a whole was 0.7% slower. So the planner leaves them to the search.
+static bool bulk_possible(const TileCand& c, int EA, const ttcb_tuning& tu, bool shift) {
   return tu.bulk_copies == 1 && tu.vec != 1 && (tu.tile_variant == 0 || tu.tile_variant == 3) &&
          (shift || c.vecA * EA == 16);
 }
@@ -580,8 +585,9 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   // (fp32) or LA / 2 (fp64) narrow ones. Run s then sits at s * shiftW + (segA[s] mod V).
   const int VM = 16 / EA;
   const bool shift = wants_shifted_runs(c, EA, p->tuning);
-  // bulk copies keep each run contiguous: the padding period is then a multiple of the run
-  const bool bulk = wants_bulk_copies(c, EA, p->tuning, shift);
+  // bulk copies of plain runs need padding points that split runs into equal pieces (sigma a
+  // multiple or a divisor of LA); decided below with the layout
+  bool bulk = bulk_possible(c, EA, p->tuning, shift);
   const int64_t CM = shift ? (2 * VM - 3 + c.LA) / VM + 1 : 0;  // chunk slots per run
   int64_t shiftW = CM * VM;
   auto staged_shift = [&](int64_t pp, int64_t W) {
@@ -645,26 +651,49 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
       }
       shiftW += best_pad;
     }
-    for (int64_t sg : sigmas) {
-      if (shift || best_cost == ideal) break;
-      if (bulk && sg % c.LA != 0) continue;
-      sigma = sg;
-      for (int k = 0; k <= 8; ++k) {
-        const int64_t cand = (int64_t)k * c.vecA;
-        if (k && (cand > 32 || cand > sg)) break;
-        if ((P - 1) / sg * cand + P > 65535) continue;
-        const int64_t cc = gather_cost(cand);
-        if (best_cost < 0 || cc < best_cost) {
-          best_cost = cc;
-          best_sigma = sg;
-          best_pad = cand;
+    // the (period, pad) pair with the fewest conflicts; with min_piece > 0 only periods that cut the
+    // runs into equal pieces of at least min_piece elements (bulk copies)
+    auto search = [&](int64_t min_piece, int64_t& out_cost, int64_t& out_sigma, int64_t& out_pad) {
+      out_cost = -1;
+      out_sigma = c.LA;
+      out_pad = 0;
+      for (int64_t sg : sigmas) {
+        if (out_cost == ideal) break;
+        if (min_piece > 0 && ((sg % c.LA != 0 && c.LA % sg != 0) || std::min<int64_t>(sg, c.LA) < min_piece)) continue;
+        sigma = sg;
+        for (int k = 0; k <= 8; ++k) {
+          const int64_t cand = (int64_t)k * c.vecA;
+          if (k && (cand > 32 || cand > sg)) break;
+          if ((P - 1) / sg * cand + P > 65535) continue;
+          const int64_t cc = gather_cost(cand);
+          if (out_cost < 0 || cc < out_cost) {
+            out_cost = cc;
+            out_sigma = sg;
+            out_pad = cand;
+          }
+          if (out_cost == ideal) break;
         }
-        if (best_cost == ideal) break;
+      }
+    };
+    if (!shift) {
+      search(0, best_cost, best_sigma, best_pad);
+      if (bulk) {
+        // the fewest conflicts among the periods that cut runs into whole 16-byte pieces
+        int64_t bc = -1, bs = c.LA, bp = 0;
+        search(1, bc, bs, bp);
+        if (bc >= 0) {
+          best_cost = bc;
+          best_sigma = bs;
+          best_pad = bp;
+        } else {
+          bulk = false;
+        }
       }
     }
     sigma = shift ? c.LA : best_sigma;
     padA = shift ? 0 : best_pad;
   }
+  const int64_t bulk_pieces = (bulk && !shift && sigma < c.LA) ? c.LA / sigma : 1;
   const int64_t staged_size = shift ? (P / c.LA) * shiftW : staged(P - 1, padA) + 1;
   std::vector<uint16_t> gtab(P);
   for (int64_t q = 0; q < P; ++q)
@@ -685,6 +714,8 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   td.shiftW = (int32_t)(shift ? shiftW : 0);
   td.shiftCM = (int32_t)CM;
   td.bulkA = bulk ? 1 : 0;
+  td.bulk_pieces = (int32_t)bulk_pieces;
+  td.divPieces = make_fastdiv((uint32_t)bulk_pieces);
   td.divCM = make_fastdiv((uint32_t)std::max<int64_t>(CM, 1));
   td.P = (int32_t)P;
   td.LA = (int32_t)c.LA;
@@ -1056,7 +1087,7 @@ ttcb_status plan_build_host(ttcb_plan* p, std::string& err) {
   if (p->shape_only) {
     p->vecA = wants_shifted_runs(best, EA, p->tuning) ? 16 / EA : best.vecA;
     p->shape_shifted = wants_shifted_runs(best, EA, p->tuning);
-    p->shape_bulk = wants_bulk_copies(best, EA, p->tuning, p->shape_shifted);
+    p->shape_bulk = bulk_possible(best, EA, p->tuning, p->shape_shifted);
     p->vecB = best.vecB;
     p->est_cost = best.cost;
     // the staged kernel's ring depth and CTAs per SM, from the staged layout's usual size (the bank
