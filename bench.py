@@ -76,7 +76,7 @@ def parse(argv=None):
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-tuning", default="search", choices=["search", "default"],
                     help="per-problem schedules: measured search (the autotuner) or the planner default")
-    ap.add_argument("--selector-cases", type=int, default=12,
+    ap.add_argument("--selector-cases", type=int, default=40,
                     help="held-out problems for the learned selector's fresh head to head")
     return ap.parse_args(argv)
 
