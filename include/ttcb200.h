@@ -95,6 +95,9 @@ typedef struct {
                             piece (cp.async.bulk into the stage, completion counted on an
                             mbarrier) where the runs allow it (16-byte aligned runs, or shifted
                             runs); 0 or -1 = per-thread 16-byte copies                          */
+  int32_t lane_map;      /* staged tile kernel, register path: 0 = planner's choice (a warp takes
+                            B vectors from several B runs when that lowers the gather's bank
+                            conflicts), -1 = never (a warp takes 32 consecutive B vectors)      */
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

@@ -109,8 +109,48 @@ def parse_tile(b):
     o = L["off_shiftA"]
     t["shiftA"], t["shiftW"], t["shiftCM"], t["bulkA"] = _i32(b, o), _i32(b, o + 4), _i32(b, o + 8), _i32(b, o + 12)
     t["bulk_pieces"] = _i32(b, o + 16 + L["fastdiv_size"])
+    t["map_log2s"], t["map_nx"], t["map_nbx"] = (_i32(b, o + 20 + L["fastdiv_size"]), _i32(b, o + 24 + L["fastdiv_size"]),
+                                                 _i32(b, o + 28 + L["fastdiv_size"]))
     t["divPieces"] = _fd(b, o + 32 + L["fastdiv_size"])
+    t["map_vb"], t["map_ny"], t["map_nslots"] = (_i32(b, o + 32 + 2 * L["fastdiv_size"]),
+                                                 _i32(b, o + 36 + 2 * L["fastdiv_size"]),
+                                                 _i32(b, o + 40 + 2 * L["fastdiv_size"]))
     return t
+
+
+def lane_map_vectors(t, nslots):
+    """The staged kernel's register-path lane map (TileDesc::map_log2s): the B vector that thread
+    slot i (warp i / 32, lane i mod 32) takes, for i in 0..nslots-1 (-1: none)."""
+    i = np.arange(nslots, dtype=np.int64)
+    if t["map_log2s"] < 0:
+        return np.where(i * max(t.get("map_vb", 1), 1) < t["P"], i, -1)
+    ls, nbx, nx = t["map_log2s"], t["map_nbx"], t["map_nx"]
+    w, l = i >> 5, i & 31
+    y = (w // nbx) * (32 >> ls) + (l >> ls)
+    v = (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + nx * y
+    return np.where((y < t["map_ny"]) & (i < t["map_nslots"]), v, -1)
+
+
+def check_lane_map(t, EB):
+    """A lane map must give every B vector to exactly one thread slot within the register path's
+    1024 slots, keep each group of map_s lanes on consecutive vectors of one B run, and give each
+    group at least one whole 32-byte sector; the map's sizes must agree with the tile."""
+    if t["map_log2s"] < 0:
+        return
+    vb = t["map_vb"]
+    s = 1 << t["map_log2s"]
+    nvB = t["P"] // vb
+    rows = 32 // s
+    assert t["LB"] % vb == 0 and t["map_nx"] == t["LB"] // vb and t["map_nbx"] * s == t["map_nx"]
+    assert t["map_ny"] == t["P"] // t["LB"]
+    assert t["map_nslots"] == t["map_nbx"] * ((t["map_ny"] + rows - 1) // rows) * 32 <= 1024
+    assert s * vb * EB >= 32, "a lane group writes less than a 32-byte sector"
+    v = lane_map_vectors(t, 1024)
+    got = v[v >= 0]
+    assert np.array_equal(np.sort(got), np.arange(nvB)), "the lane map is not a bijection"
+    g = v[: t["map_nslots"]].reshape(-1, s)
+    g = g[g[:, 0] >= 0]
+    assert (np.diff(g, axis=1) == 1).all() and ((g[:, 0] % t["map_nx"]) + s <= t["map_nx"]).all()
 
 
 def check_bulk_layout(t, EA):

@@ -63,7 +63,8 @@ class Tuning(ctypes.Structure):
                 ("streaming", ctypes.c_int32), ("tile_variant", ctypes.c_int32), ("ragged", ctypes.c_int32),
                 ("raster_lo", ctypes.c_int32), ("raster_hi", ctypes.c_int32), ("stages", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("round_robin", ctypes.c_int32),
-                ("shifted_runs", ctypes.c_int32), ("bulk_copies", ctypes.c_int32)]
+                ("shifted_runs", ctypes.c_int32), ("bulk_copies", ctypes.c_int32),
+                ("lane_map", ctypes.c_int32)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":

@@ -87,8 +87,21 @@ struct TileDesc {
   int32_t bulkA;
   FastDiv divCM;      // divisor shiftCM
   int32_t bulk_pieces;  // bulk copies per A run (plain runs)
-  int32_t bulk_pad_[3];
+  // Lane map of the staged kernel's register path (when its B vector width is map_vb): a warp's
+  // 32 lanes take map_s consecutive B vectors from each of 32 / map_s consecutive B runs instead of
+  // 32 consecutive vectors, so that the gathers of one load fall into more banks (lanes in
+  // different runs read different A positions). Warp w covers columns (w mod map_nbx) * map_s ..
+  // + map_s - 1 of rows (w / map_nbx) * (32 / map_s) .. of the (B vectors per run) x (B runs) grid;
+  // lane l takes column offset l mod map_s, row offset l / map_s. The last footprint row may reach
+  // past the tile's B runs: those slots take no vector.
+  int32_t map_log2s;  // log2 map_s, or -1: no map (lane i of the block takes vector i)
+  int32_t map_nx;     // B vectors per B run (LB / map_vb)
+  int32_t map_nbx;    // warp footprints across the B vectors of a run (map_nx / map_s)
   FastDiv divPieces;  // divisor bulk_pieces
+  int32_t map_vb;     // the B vector width the map is planned for
+  int32_t map_ny;     // B runs in the tile; thread slots whose row is past them take no vector
+  int32_t map_nslots; // thread slots the map spans (map_nbx * ceil(map_ny / (32 / map_s)) * 32)
+  int32_t map_pad_;
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
 };
 

@@ -633,19 +633,35 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   // the tile shifts x for which each of the thread's A copies is made: x in [lo, hi), 4-bit fields
   // (lo + 1, hi) per copy; without shifted runs a copy is made at x = 0 when it exists
   uint32_t lohi = 0;
+  // the register path's lane map (TileDesc::map_log2s): the B vector of thread slot i
+  const bool lane_map = REG && d.map_log2s >= 0 && d.map_vb == VB;
+  // (-1: the slot takes no vector)
+  auto vec_of = [&](int i) -> int {
+    if (!lane_map) return i < nvB ? i : -1;
+    if (i >= d.map_nslots) return -1;
+    const int w = i >> 5, l = i & 31, ls = d.map_log2s, nbx = d.map_nbx;
+    const int y = (w / nbx) * (32 >> ls) + (l >> ls);
+    return y < d.map_ny ? (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + d.map_nx * y : -1;
+  };
+  uint32_t vmask = 0;  // register path: bit u set when the thread's slot u takes a B vector
+  // BETA, register path: the B stage byte offset of each of the thread's B vectors (two per register)
+  uint32_t qb[REG && BETA ? (kRegVec + 1) / 2 : 1];
+#pragma unroll
+  for (int e = 0; e < (int)(sizeof(qb) / sizeof(qb[0])); ++e) qb[e] = 0;
 #pragma unroll
   for (int e = 0; e < kGp; ++e) gp[e] = 0;
   if (reg_pos) {
 #pragma unroll
     for (int u = 0; u < kVecB; ++u) {
-      const int i = tid + u * kThreads;
-      if (i < nvB) {
+      const int vi = vec_of(tid + u * kThreads);
+      if (vi >= 0) {
 #pragma unroll
         for (int j = 0; j < VB; ++j) {
           const int e = u * VB + j;
-          const uint32_t v = (uint32_t)ggtab[i * VB + j] * (REG ? (uint32_t)sizeof(TA) : 1u);
+          const uint32_t v = (uint32_t)ggtab[vi * VB + j] * (REG ? (uint32_t)sizeof(TA) : 1u);
           gp[e >> 1] |= (e & 1) ? (v << 16) : v;
         }
+        if constexpr (REG && BETA) qb[u >> 1] |= ((uint32_t)(vi * VB * (int)sizeof(TB))) << ((u & 1) * 16);
       }
     }
   }
@@ -679,13 +695,20 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
         dA[u >> 1] |= ((uint32_t)(p + sp * padA) * (uint32_t)sizeof(TA)) << ((u & 1) * 16);
         lohi |= (1u | (1u << 4)) << (8 * u);  // x = 0 is in [0, 1)
       }
-      if (i < nvB) {
-        const int q = i * VB;
+      const int vi = vec_of(i);
+      if (vi >= 0) {
+        const int q = vi * VB;
         const int s = (int)fdiv((uint32_t)q, divLB);
         rB[u] = (int32_t)(gB[s] + (q - s * LB));
+        vmask |= 1u << u;
       }
     }
   }
+  // B stage byte offset of the thread's u-th B vector (register path with beta)
+  auto qb_of = [&](int u) -> uint32_t {
+    if constexpr (REG && BETA) return (qb[u >> 1] >> ((u & 1) * 16)) & 0xffffu;
+    return 0u;
+  };
 
   const uint32_t ntiles = (uint32_t)d.nfull;  // the ragged tiles are the ragged-tile kernel's
   const uint32_t G = gridDim.x;
@@ -752,10 +775,8 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       if constexpr (BETA) {
         if constexpr (REG) {
 #pragma unroll
-          for (int u = 0; u < kRegVec; ++u) {
-            const int i = tid + u * kThreads;
-            if (i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
-          }
+          for (int u = 0; u < kRegVec; ++u)
+            if ((vmask >> u) & 1u) cp_async<VB * sizeof(TB)>(sbB + qb_of(u), Bt + rB[u]);
         } else {
           const int LB = d.LB;
           const FastDiv divLB = d.divLB;
@@ -771,11 +792,10 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     if constexpr (REG) {
 #pragma unroll
       for (int u = 0; u < kRegVec; ++u) {
-        const int i = tid + u * kThreads;
         const uint32_t f = lohi >> (8 * u);
         if (x + 1 >= (int)(f & 15u) && x < (int)((f >> 4) & 15u))
           cp_async<VA * sizeof(TA)>(sb + ((dA[u >> 1] >> ((u & 1) * 16)) & 0xffffu), At + rA[u]);
-        if (BETA && i < nvB) cp_async<VB * sizeof(TB)>(sbB + (uint32_t)(i * VB * sizeof(TB)), Bt + rB[u]);
+        if (BETA && ((vmask >> u) & 1u)) cp_async<VB * sizeof(TB)>(sbB + qb_of(u), Bt + rB[u]);
       }
     } else {
       const int LA = d.LA, LB = d.LB, padA = d.padA;
@@ -929,11 +949,11 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       if constexpr (REG) {
 #pragma unroll
         for (int u = 0; u < kRegVec; ++u) {
-          const int i = tid + u * kThreads;
-          if (i < nvB) {
+          if ((vmask >> u) & 1u) {
             uint32_t off[VB];
             reg_pos_of(u, off);
-            out_vec(stage, sB, i * VB, off, Bt + rB[u]);
+            out_vec(stage, reinterpret_cast<const TB*>(reinterpret_cast<const unsigned char*>(sB) + qb_of(u)), 0, off,
+                    Bt + rB[u]);
           }
         }
       } else {

@@ -524,6 +524,7 @@ static bool bulk_possible(const TileCand& c, int EA, const ttcb_tuning& tu, bool
 
 static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   const FusedProblem& f = p->f;
+  const int EB_ = dtype_bytes(p->tb);
   std::vector<int> aord, bord;
   tile_orders(f, c.ext, aord, bord);
   // tile strides in A order / B order
@@ -594,8 +595,24 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
     const int64_t s = pp / c.LA;
     return s * W + (((segA[s] % VM) + VM) % VM) + (pp - s * c.LA);
   };
+  // The register path's lane map (TileDesc::map_log2s): with map_s > 0 a warp takes map_s B vectors
+  // from each of 32 / map_s consecutive B runs; vec_of gives the B vector of thread slot i.
+  const int64_t map_nx = c.LB / c.vecB, map_ny = P / c.LB;
+  int map_s = 0;
+  // -1: a slot past the tile's B runs
+  auto vec_of = [&](int64_t i) -> int64_t {
+    if (!map_s) return i * c.vecB < P ? i : -1;
+    const int64_t w = i >> 5, l = i & 31, nbx = map_nx / map_s;
+    const int64_t y = (w / nbx) * (32 / map_s) + l / map_s;
+    return y < map_ny ? (w % nbx) * map_s + (l % map_s) + map_nx * y : -1;
+  };
+  auto map_slots = [&](int ms) -> int64_t {
+    const int64_t rows = 32 / ms;
+    return (map_nx / ms) * ((map_ny + rows - 1) / rows) * 32;
+  };
   // A warp's 8-byte loads are served per half-warp and its 16-byte loads per quarter-warp, so the
-  // wavefronts of one load are the sum over those lane groups of the busiest bank's count.
+  // wavefronts of one load are the sum over those lane groups of the busiest bank's count. The cost
+  // is the wavefronts beyond one per lane group (0 = no conflicts), over the first four warps.
   const int group = 32 / EAw;
   auto gather_cost = [&](int64_t padA) {
     int64_t cost = 0;
@@ -606,16 +623,16 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
           int cnt[32] = {0};
           int mx = 0;
           for (int lane = g0; lane < g0 + group; ++lane) {
-            int64_t i = (int64_t)w * 32 + lane;
-            if (i * vb >= P) continue;
-            int64_t word = (shift ? staged_shift(p_of_q[i * vb + j], shiftW + padA)
-                                  : staged(p_of_q[i * vb + j], padA)) * EAw;
+            const int64_t v = vec_of((int64_t)w * 32 + lane);
+            if (v < 0) continue;
+            int64_t word = (shift ? staged_shift(p_of_q[v * vb + j], shiftW + padA)
+                                  : staged(p_of_q[v * vb + j], padA)) * EAw;
             for (int x = 0; x < EAw; ++x) {
               int b = (int)((word + x) & 31);
               mx = std::max(mx, ++cnt[b]);
             }
           }
-          cost += mx;
+          cost += mx > 0 ? mx - 1 : 0;
         }
       }
     }
@@ -631,11 +648,7 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
         if (tsA[d] > 1 && m * tsA[d] < P && (m * tsA[d]) % c.vecA == 0) sigmas.push_back(m * tsA[d]);
     for (int64_t k = c.vecA; k <= 64 && k < P; k += c.vecA) sigmas.push_back(k);
     // one wavefront per lane group and load is the floor; stop searching once it is reached
-    int64_t ideal = 0;
-    for (int w = 0; w < 4; ++w)
-      for (int j = 0; j < c.vecB; ++j)
-        for (int g0 = 0; g0 < 32; g0 += group)
-          if (((int64_t)w * 32 + g0) * c.vecB < P) ++ideal;
+    const int64_t ideal = 0;
     int64_t best_cost = -1, best_sigma = c.LA, best_pad = 0;
     if (shift) {
       // the run stride: the chunk slots plus 0..8 chunks of padding, the fewest conflicts
@@ -689,6 +702,29 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
           bulk = false;
         }
       }
+      // Lane maps, when the layout alone leaves conflicts and the tile can take the register path
+      // (every thread's B vectors in registers): the pads are multiples of the A vector, so lanes
+      // whose A positions differ by multiples of a larger power of two meet in the same banks
+      // whatever the layout; lanes spread over several B runs read different A positions. Each
+      // lane group keeps at least one whole 32-byte sector of its B run, so stores stay complete.
+      const bool reg_shape = P / c.vecA <= 4 * ttcb::kThreads && P / c.vecB <= 4 * ttcb::kThreads &&
+                             P * EB_ < 65536 && p->tuning.lane_map >= 0;
+      if (best_cost > ideal && reg_shape) {
+        int best_map = 0;
+        for (int ms = 1; ms <= 16; ms *= 2) {
+          if ((int64_t)ms * c.vecB * EB_ < 32 || map_nx % ms != 0 || map_slots(ms) > 4 * ttcb::kThreads) continue;
+          map_s = ms;
+          int64_t mc = -1, msg = c.LA, mp = 0;
+          search(bulk ? 1 : 0, mc, msg, mp);
+          if (mc >= 0 && mc < best_cost) {
+            best_cost = mc;
+            best_sigma = msg;
+            best_pad = mp;
+            best_map = ms;
+          }
+        }
+        map_s = best_map;
+      }
     }
     sigma = shift ? c.LA : best_sigma;
     padA = shift ? 0 : best_pad;
@@ -715,6 +751,12 @@ static void build_tile_desc(ttcb_plan* p, const TileCand& c, int EA) {
   td.shiftCM = (int32_t)CM;
   td.bulkA = bulk ? 1 : 0;
   td.bulk_pieces = (int32_t)bulk_pieces;
+  td.map_log2s = map_s ? __builtin_ctz((unsigned)map_s) : -1;
+  td.map_nx = (int32_t)(map_s ? map_nx : 0);
+  td.map_nbx = (int32_t)(map_s ? map_nx / map_s : 0);
+  td.map_vb = map_s ? c.vecB : 0;
+  td.map_ny = (int32_t)(map_s ? map_ny : 0);
+  td.map_nslots = (int32_t)(map_s ? map_slots(map_s) : 0);
   td.divPieces = make_fastdiv((uint32_t)bulk_pieces);
   td.divCM = make_fastdiv((uint32_t)std::max<int64_t>(CM, 1));
   td.P = (int32_t)P;
@@ -1204,7 +1246,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
       << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
       << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm
-      << ",\"shifted_runs\":" << t->shiftA << ",\"bulk\":" << t->bulkA << ",\"claims\":" << (p->claim_words ? 1 : 0)
+      << ",\"shifted_runs\":" << t->shiftA << ",\"bulk\":" << t->bulkA << ",\"lane_map\":" << (t->map_log2s >= 0 ? (1 << t->map_log2s) : 0) << ",\"claims\":" << (p->claim_words ? 1 : 0)
       << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";
