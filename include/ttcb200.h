@@ -95,9 +95,10 @@ typedef struct {
                             piece (cp.async.bulk into the stage, completion counted on an
                             mbarrier) where the runs allow it (16-byte aligned runs, or shifted
                             runs); 0 or -1 = per-thread 16-byte copies                          */
-  int32_t lane_map;      /* staged tile kernel, register path: 0 = planner's choice (a warp takes
-                            B vectors from several B runs when that lowers the gather's bank
-                            conflicts), -1 = never (a warp takes 32 consecutive B vectors)      */
+  int32_t lane_map;      /* staged tile kernel, register path: 1 = a warp takes B vectors from
+                            several B runs (in their order, or sorted by A position) when the
+                            planner's model finds fewer bank conflicts in the gather that way;
+                            0 or -1 = a warp takes 32 consecutive B vectors                     */
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

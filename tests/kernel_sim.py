@@ -115,6 +115,9 @@ def parse_tile(b):
     t["map_vb"], t["map_ny"], t["map_nslots"] = (_i32(b, o + 32 + 2 * L["fastdiv_size"]),
                                                  _i32(b, o + 36 + 2 * L["fastdiv_size"]),
                                                  _i32(b, o + 40 + 2 * L["fastdiv_size"]))
+    t["off_runs"] = _i32(b, o + 44 + 2 * L["fastdiv_size"])
+    t["runs"] = (np.frombuffer(b, dtype=np.uint16, count=t["map_ny"], offset=t["off_runs"]).astype(np.int64)
+                 if t["off_runs"] else None)
     return t
 
 
@@ -127,8 +130,10 @@ def lane_map_vectors(t, nslots):
     ls, nbx, nx = t["map_log2s"], t["map_nbx"], t["map_nx"]
     w, l = i >> 5, i & 31
     y = (w // nbx) * (32 >> ls) + (l >> ls)
-    v = (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + nx * y
-    return np.where((y < t["map_ny"]) & (i < t["map_nslots"]), v, -1)
+    ok = (y < t["map_ny"]) & (i < t["map_nslots"])
+    run = y if t["runs"] is None else t["runs"][np.where(ok, y, 0)]
+    v = (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + nx * run
+    return np.where(ok, v, -1)
 
 
 def check_lane_map(t, EB):
@@ -145,6 +150,8 @@ def check_lane_map(t, EB):
     assert t["map_ny"] == t["P"] // t["LB"]
     assert t["map_nslots"] == t["map_nbx"] * ((t["map_ny"] + rows - 1) // rows) * 32 <= 1024
     assert s * vb * EB >= 32, "a lane group writes less than a 32-byte sector"
+    if t["runs"] is not None:
+        assert np.array_equal(np.sort(t["runs"]), np.arange(t["map_ny"])), "the run order is not a permutation"
     v = lane_map_vectors(t, 1024)
     got = v[v >= 0]
     assert np.array_equal(np.sort(got), np.arange(nvB)), "the lane map is not a bijection"

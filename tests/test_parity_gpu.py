@@ -100,7 +100,7 @@ TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"loop_order": 3}, 
            {"streaming": 1}, {"round_robin": 1}, {"stages": 3}, {"stages": 7}, {"ctas_per_sm": 1},
            {"stages": 6, "ctas_per_sm": 2}, {"round_robin": 1, "blocks": 5}, {"round_robin": -1},
            {"round_robin": -1, "blocks": 5}, {"bulk_copies": 1}, {"bulk_copies": 1, "round_robin": -1},
-           {"bulk_copies": 1, "shifted_runs": 1}, {"lane_map": -1}]
+           {"bulk_copies": 1, "shifted_runs": 1}, {"lane_map": 1}]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS, ids=[str(t) for t in TUNINGS])
@@ -403,18 +403,18 @@ LANE_MAPS = [([1, 0, 2, 3], [48, 3, 48, 29]), ([1, 0], [54, 48]), ([2, 3, 1, 0],
 
 @pytest.mark.parametrize("dtype", ["s", "d", "c", "sd", "ds"])
 def test_lane_maps(dtype):
-    """Plans whose register path takes B vectors from several B runs per warp (lane maps, chosen by
-    the planner against the gather's bank conflicts), including maps whose last footprint row
-    reaches past the tile's runs: bit for bit against the oracle for beta = 0 and beta != 0, with
-    claimed tiles, bulk copies, and with the map turned off."""
+    """Plans whose register path takes B vectors from several B runs per warp (lane_map = 1: maps
+    the planner picks against the gather's bank conflicts, in natural or A-sorted run order),
+    including maps whose last footprint row reaches past the tile's runs: bit for bit against the
+    oracle for beta = 0 and beta != 0, with claimed tiles, bulk copies and round-robin tiles."""
     used = 0
     for perm, size in LANE_MAPS:
         for beta in (0.0, -0.5):
-            desc = check_case(perm, size, dtype, 1.5, beta)
+            desc = check_case(perm, size, dtype, 1.5, beta, tuning={"lane_map": 1})
             used += int((desc.get("tile") or {}).get("lane_map", 0) > 0)
-            check_case(perm, size, dtype, 1.5, beta, tuning={"round_robin": -1, "blocks": 7})
-            check_case(perm, size, dtype, 1.5, beta, tuning={"bulk_copies": 1})
-            check_case(perm, size, dtype, 1.5, beta, tuning={"lane_map": -1})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"lane_map": 1, "round_robin": -1, "blocks": 7})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"lane_map": 1, "bulk_copies": 1})
+            check_case(perm, size, dtype, 1.5, beta, tuning={"lane_map": 1, "round_robin": 1, "stages": 5})
     assert used > 0
 
 

@@ -441,18 +441,19 @@ def test_bulk_copy_layout_replay():
 
 
 def test_lane_maps():
-    """Lane maps of the staged kernel's register path (a warp takes B vectors from several B runs
-    when that lowers the gather's bank conflicts): on random problems with short B runs, every map
-    is a bijection of the tile's B vectors whose lane groups each write whole 32-byte sectors of one
-    B run (kernel_sim.check_lane_map); the planner's conflict model scores the chosen map below the
-    plain order; lane_map = -1 turns maps off; and the element mapping equals the oracle's."""
+    """Lane maps of the staged kernel's register path (a warp takes B vectors from several B runs,
+    in their natural order or sorted by A position, when that lowers the gather's bank conflicts):
+    on random problems, every map is a bijection of the tile's B vectors whose lane groups each
+    write whole 32-byte sectors of one B run, and every run order a permutation
+    (kernel_sim.check_lane_map); without lane_map = 1 no plan has one; and the element mapping
+    equals the oracle's."""
     rng = np.random.default_rng(21)
-    maps = 0
+    maps = sorted_runs = 0
     for it in range(120):
         perm, size, lda, ldb = _random_problem(rng, max_rank=5, max_ext=40, pad=False)
         for dtype in ("s", "d", "sd"):
             try:
-                kind, b = kernel_sim.host_desc(perm, size, dtype, it % 2 == 1)
+                kind, b = kernel_sim.host_desc(perm, size, dtype, it % 2 == 1, tuning={"lane_map": 1})
             except TTCError:
                 continue
             if kind != 1:
@@ -461,12 +462,13 @@ def test_lane_maps():
             if t["map_log2s"] < 0:
                 continue
             maps += 1
+            sorted_runs += int(t["runs"] is not None)
             EB = {"s": 4, "d": 8}[dtype[-1]]
             kernel_sim.check_lane_map(t, EB)
-            _, b2 = kernel_sim.host_desc(perm, size, dtype, it % 2 == 1, tuning={"lane_map": -1})
+            _, b2 = kernel_sim.host_desc(perm, size, dtype, it % 2 == 1)
             assert kernel_sim.parse_tile(b2)["map_log2s"] < 0
             if maps <= 12:
-                _, (a, bb) = kernel_sim.simulate(perm, size, dtype, it % 2 == 1)
+                _, (a, bb) = kernel_sim.simulate(perm, size, dtype, it % 2 == 1, tuning={"lane_map": 1})
                 wa, wb = _oracle_pairs(perm, size, None, None)
                 assert dict(zip(bb.tolist(), a.tolist())) == dict(zip(wb.tolist(), wa.tolist()))
-    assert maps >= 10, maps
+    assert maps >= 10 and sorted_runs >= 2, (maps, sorted_runs)

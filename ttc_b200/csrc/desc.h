@@ -101,7 +101,10 @@ struct TileDesc {
   int32_t map_vb;     // the B vector width the map is planned for
   int32_t map_ny;     // B runs in the tile; thread slots whose row is past them take no vector
   int32_t map_nslots; // thread slots the map spans (map_nbx * ceil(map_ny / (32 / map_s)) * 32)
-  int32_t map_pad_;
+  // byte offset (from the descriptor start) of the map's run order, uint16_t[map_ny]: footprint
+  // row y takes B run runs[y] (the runs sorted by the A position of their first element, so that
+  // a warp's rows start at neighbouring A positions); 0: row y takes run y
+  int32_t off_runs;
   // followed by: int64_t segA[nsegA]; int64_t segB[nsegB]; uint16_t perm_tab[P] (slots)
 };
 

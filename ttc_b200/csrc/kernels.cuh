@@ -641,7 +641,9 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
     if (i >= d.map_nslots) return -1;
     const int w = i >> 5, l = i & 31, ls = d.map_log2s, nbx = d.map_nbx;
     const int y = (w / nbx) * (32 >> ls) + (l >> ls);
-    return y < d.map_ny ? (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + d.map_nx * y : -1;
+    if (y >= d.map_ny) return -1;
+    const int run = d.off_runs ? (int)reinterpret_cast<const uint16_t*>(base + d.off_runs)[y] : y;
+    return (w % nbx) * (1 << ls) + (l & ((1 << ls) - 1)) + d.map_nx * run;
   };
   uint32_t vmask = 0;  // register path: bit u set when the thread's slot u takes a B vector
   // BETA, register path: the B stage byte offset of each of the thread's B vectors (two per register)
