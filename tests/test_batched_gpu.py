@@ -68,6 +68,42 @@ def test_batched_beta_mixed_kernels_and_dtypes():
             assert_bitexact(bb.cpu().numpy(), w, f"{dtype} problem {k}")
 
 
+@pytest.mark.parametrize("dtype", ["s", "d"])
+def test_batched_ragged_tiles_and_vector_widths(dtype):
+    """Batched problems whose ragged tiles go element-wise inside the batch's ring (ragged = 1), next to
+    problems with every access-width pair (full, half and scalar vectors, from the problems' own
+    alignment and from vec = 1), small tiles with many tiles per problem, beta = 0 and beta != 0: bit
+    for bit against the oracle."""
+    import torch
+    from ttc_b200 import Plan
+    from ttc_b200.batched import Batch
+    rng = np.random.default_rng(11)
+    tmap = {"s": torch.float32, "d": torch.float64}
+    for beta in (0.0, -0.5):
+        plans, As, Bs, wants = [], [], [], []
+        for k in range(60):
+            r = int(rng.integers(2, 5))
+            size = [int(x) for x in rng.integers(3, 70, r)]
+            if int(np.prod(size)) > 400000:
+                size[-1] = 3
+            perm = [int(x) for x in rng.permutation(r)]
+            n = int(np.prod(size))
+            a = uniform(n, dtype, 500 + k)
+            b = uniform(n, dtype, 900 + k)
+            wants.append(oracle.transpose(a, b.copy(), perm, size, 1.5, beta, dtype=dtype))
+            tu = [{"ragged": 1}, {"ragged": 1, "tile_elems": 256}, {"vec": 1}, {}, {"tile_elems": 512}][k % 5]
+            plans.append(Plan(perm, size, dtype, beta != 0, tuning=tu))
+            As.append(torch.from_numpy(a).cuda())
+            Bs.append(torch.from_numpy(b).cuda())
+        batch = Batch(plans, As, Bs, alpha=1.5, beta=beta)
+        batch.launch()
+        batch.check_status()
+        torch.cuda.synchronize()
+        for k, (bb, w) in enumerate(zip(Bs, wants)):
+            assert_bitexact(bb.cpu().numpy(), w, f"{dtype} beta={beta} problem {k}")
+        batch.close()
+
+
 def test_batch_rejects_mixed_types():
     from ttc_b200 import Plan, TTCError
     from ttc_b200.batched import Batch
