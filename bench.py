@@ -68,7 +68,8 @@ def parse(argv=None):
     ap.add_argument("--schedule", default="learned", choices=["default", "learned"],
                     help="sweep: the planner's default schedule per case, or the learned selector's choice "
                          "(chosen before the timed region: its top-1 on a large predicted gain over the "
-                         "planner default, the faster of the two, timed, on a moderate one)")
+                         "planner default, the fastest of its top candidates and the default, timed, on a "
+                         "moderate one)")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
     ap.add_argument("--reps", type=int, default=3, help="case / batchcase: launches")
     ap.add_argument("--tuning", default=None, help="case: a schedule (JSON of ttcb_tuning fields) instead of the "
@@ -630,7 +631,7 @@ def run_sweep(args, rank, world, local):
                 "pct_of_hbm_peak": round(100 * value / world / peak, 2),
                 "config": sweep_config(len(cases), bytes_per_step, world),
                 "schedules": schedule_note or ("learned selector (top-1 on a large predicted gain over the planner "
-                                               "default, timed against it on a moderate one)" if args.schedule == "learned"
+                                               "default; its top candidates timed against it on a moderate one)" if args.schedule == "learned"
                                                else "planner default"),
                 "schedule_seconds": round(t_sel, 1),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

@@ -100,7 +100,8 @@ def test_trained_selector_beats_the_planner_default():
     """What the trained network gains over the method without it, on fresh timings of held-out
     problems (the first 40 of the held-out seed; no stored timing is reused): every candidate is timed
     (TTC's exhaustive method), then the search's winner, the network's top-1, the selector's choice
-    (under the model's policy: the default, the top-1, or the faster of the two, timed) and the
+    (under the model's policy: the default, the top-1, or the fastest of its top k and the default,
+    timed) and the
     planner default alone are re-timed alternately. The selector keeps a larger share of the winner's
     GB/s than the planner default, and tunes in a small fraction of the search's time."""
     import ttc_b200.workloads as wl
