@@ -99,6 +99,8 @@ typedef struct {
                             several B runs (in their order, or sorted by A position) when the
                             planner's model finds fewer bank conflicts in the gather that way;
                             0 or -1 = a warp takes 32 consecutive B vectors                     */
+  int32_t claim_group;   /* staged tile kernel with claimed tiles: consecutive tiles per claim
+                            (1..64); 0 = planner's choice (2)                                   */
 } ttcb_tuning;
 
 typedef struct ttcb_plan ttcb_plan;

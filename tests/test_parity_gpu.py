@@ -99,7 +99,8 @@ TUNINGS = [{"vec": 1}, {"loop_order": 1}, {"loop_order": 2}, {"loop_order": 3}, 
            {"tile_elems": 8192}, {"run_bytes": 128}, {"run_bytes": 2048}, {"kernel": 1}, {"streaming": -1},
            {"streaming": 1}, {"round_robin": 1}, {"stages": 3}, {"stages": 7}, {"ctas_per_sm": 1},
            {"stages": 6, "ctas_per_sm": 2}, {"round_robin": 1, "blocks": 5}, {"round_robin": -1},
-           {"round_robin": -1, "blocks": 5}, {"bulk_copies": 1}, {"bulk_copies": 1, "round_robin": -1},
+           {"round_robin": -1, "blocks": 5}, {"round_robin": -1, "claim_group": 3},
+           {"round_robin": -1, "claim_group": 8, "blocks": 3}, {"bulk_copies": 1}, {"bulk_copies": 1, "round_robin": -1},
            {"bulk_copies": 1, "shifted_runs": 1}, {"lane_map": 1}]
 
 

@@ -64,7 +64,7 @@ class Tuning(ctypes.Structure):
                 ("raster_lo", ctypes.c_int32), ("raster_hi", ctypes.c_int32), ("stages", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("round_robin", ctypes.c_int32),
                 ("shifted_runs", ctypes.c_int32), ("bulk_copies", ctypes.c_int32),
-                ("lane_map", ctypes.c_int32)]
+                ("lane_map", ctypes.c_int32), ("claim_group", ctypes.c_int32)]
 
     @classmethod
     def make(cls, **kw) -> "Tuning":

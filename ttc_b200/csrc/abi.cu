@@ -176,6 +176,8 @@ static ttcb_status plan_finish_device(ttcb_plan* p) {
       const int64_t tile_bytes = (int64_t)td->P * (EA + dtype_bytes(p->tb) * (p->beta_nonzero ? 2 : 1));
       const bool claims_by_default = p->tuning.round_robin == 0 && tile_bytes >= kClaimMinTileBytes &&
                                      td->nfull >= (int64_t)kClaimMinTilesPerCta * p->blocks_async;
+      // two tiles per claim: back to back over the sweep, 0.3% faster than one (three: 0.3% slower)
+      p->claim_group = p->tuning.claim_group > 0 ? std::min(p->tuning.claim_group, 64) : 2;
       if (p->tuning.round_robin == -1 || claims_by_default) {
         e = cudaMalloc(&p->claim_words, sizeof(unsigned int) * 2 * ttcb::kClaimSlots);
         if (e != cudaSuccess) {

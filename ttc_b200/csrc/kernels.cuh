@@ -572,8 +572,8 @@ constexpr size_t kAsyncStaticSmem = sizeof(TileDesc) + kInfoRing * sizeof(TileIn
 // DYN: tiles are claimed in order from a counter in global memory (sched[0]) as the CTA goes, instead
 // of the fixed round-robin blockIdx.x + k * gridDim.x. CTAs then stay on neighbouring tiles however
 // their speeds differ, so the tiles in motion stay within a narrow span of A and B, and the last
-// tiles go to whichever CTAs are free. Each claim is issued one iteration before its result is
-// used; the last CTA to finish (sched[1] counts them) sets both words back to zero for the next
+// tiles go to whichever CTAs are free. Each claim takes claim_group consecutive tiles and is issued
+// a group before its tiles are used; the last CTA to finish (sched[1] counts them) sets both words back to zero for the next
 // launch that uses them, which runs after this grid completes (stream order, and griddepcontrol.wait
 // before the first claim when the launch overlaps its predecessor).
 // a0 (shifted A runs only): A's pointer is a0 elements past a 16-byte boundary.
@@ -586,7 +586,7 @@ template <typename TA, typename TB, int VA, int VB, bool BETA, bool STREAM, bool
 __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB * sizeof(TB), BETA))
     tile_async_kernel(
     const TileDesc* __restrict__ desc, const TA* __restrict__ A, TB* __restrict__ B, TA alpha, TB beta,
-    unsigned int* __restrict__ sched, int a0, unsigned int* __restrict__ wait_status) {
+    unsigned int* __restrict__ sched, int a0, unsigned int* __restrict__ wait_status, unsigned int claim_group) {
   static_assert(!BULK || VA * sizeof(TA) == 16, "bulk copies move runs of whole 16-byte vectors");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TileDesc d;  // the descriptor header, read once per CTA
@@ -857,7 +857,9 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
   // (k - 2) every thread finished writing out before the barrier of iteration k - 1. Tiles are
   // decoded in batches (see TileInfo).
   const int D = S - 2;
-  unsigned int pending = 0;  // DYN: thread 0's claim for the tile of iteration k + D + 3
+  // DYN: thread 0 claims claim_group consecutive tiles per atomic, one group ahead: `pending` is the
+  // first tile of the next group, `cbase` of the current one, `cleft` the current group's tiles left
+  unsigned int pending = 0, cbase = 0, cleft = 0;
   uint32_t phase = 0;        // BULK: bit s = parity of the next phase of stage s's barrier
   if constexpr (BULK) {
     if (tid == 0) {
@@ -872,7 +874,7 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       unsigned int base = 0;
       if (tid == 0) {
         base = atomicAdd(&sched[0], (unsigned int)(D + 2));
-        pending = atomicAdd(&sched[0], 1u);
+        pending = atomicAdd(&sched[0], claim_group);
       }
       base = __shfl_sync(0xffffffffu, base, 0);
       if (tid < D + 2) decode_into(base + tid, info[tid]);
@@ -933,8 +935,13 @@ __global__ void __launch_bounds__(kThreads, async_min_blocks(VA * sizeof(TA), VB
       // result thread 0 needs only an iteration later (decoding here, before thread 0's own stores,
       // timed 3% faster over the 200 MiB sweep than after them)
       if (tid == 0) {
-        decode_into(pending, info[(k + D + 2) % kInfoRing]);
-        pending = atomicAdd(&sched[0], 1u);
+        if (cleft == 0) {
+          cbase = pending;
+          cleft = claim_group;
+          pending = atomicAdd(&sched[0], claim_group);
+        }
+        decode_into(cbase + (claim_group - cleft), info[(k + D + 2) % kInfoRing]);
+        --cleft;
       }
     } else {
       const uint32_t t = blockIdx.x + k * G;

@@ -82,7 +82,8 @@ static cudaError_t launch_async(const ttcb_plan* p, const void* A, void* B, cons
   const int a0 = (int)(((uintptr_t)A / sizeof(TA)) & (uintptr_t)(VA - 1));
   return cudaLaunchKernelEx(&cfg, tile_async_kernel<TA, TB, VA, VB, BETA, STREAM, REG, DYN, BULK>,
                             reinterpret_cast<const TileDesc*>(p->dev_desc), static_cast<const TA*>(A),
-                            static_cast<TB*>(B), al, be, sched, a0, BULK ? p->wait_status : nullptr);
+                            static_cast<TB*>(B), al, be, sched, a0, BULK ? p->wait_status : nullptr,
+                            (unsigned int)(p->claim_group > 0 ? p->claim_group : 1));
 }
 
 template <int VA, int VB, bool REG, bool DYN, bool BULK>

@@ -1272,7 +1272,7 @@ std::string plan_describe_json(const ttcb_plan* p) {
       << ",\"padA\":" << t->padA << ",\"sigmaA\":" << t->sigmaA << ",\"stages\":" << t->nstages
       << ",\"reg\":" << t->reg_ok << ",\"smem_async\":" << p->smem_async
       << ",\"blocks_async\":" << p->blocks_async << ",\"ctas_per_sm\":" << p->ctas_per_sm
-      << ",\"shifted_runs\":" << t->shiftA << ",\"bulk\":" << t->bulkA << ",\"lane_map\":" << (t->map_log2s >= 0 ? (1 << t->map_log2s) : 0) << ",\"claims\":" << (p->claim_words ? 1 : 0)
+      << ",\"shifted_runs\":" << t->shiftA << ",\"bulk\":" << t->bulkA << ",\"lane_map\":" << (t->map_log2s >= 0 ? (1 << t->map_log2s) : 0) << ",\"claims\":" << (p->claim_words ? 1 : 0) << ",\"claim_group\":" << p->claim_group
       << ",\"ragged_tiles\":" << (t->nrag0 + t->nrag1) << ",\"ext\":[";
     for (int d = 0; d < p->f.rank; ++d) o << (d ? "," : "") << p->tile_ext[d];
     o << "]}";

@@ -75,6 +75,7 @@ struct ttcb_plan {
   // staged kernel with claimed tiles: kClaimSlots pairs of counter words on the device (zeroed at
   // creation, reset by each launch's last CTA) and the host's running launch count
   unsigned int* claim_words = nullptr;
+  int claim_group = 1;           // tiles per claim
   void* launch_count = nullptr;  // std::atomic<unsigned int>
   // staged kernel with bulk A copies: count of stage waits that ran out of time (device word, zeroed
   // at creation; read and cleared by ttcb_plan_wait_timeouts)
