@@ -235,6 +235,8 @@ class MLP:
         self.sd = np.ones(nin, np.float32)
         self.ymu, self.ysd = 0.0, 1.0
         self.rmse = 1.0
+        # further ensemble members (same shape and normalisation); predictions average over all
+        self.extra = []
 
     def forward(self, X):
         W1, b1, W2, b2, W3, b3 = self.params
@@ -287,15 +289,28 @@ class MLP:
         return torch.from_numpy(((X - self.mu) / self.sd).astype(np.float32)).cuda()
 
     def predict(self, X: np.ndarray) -> np.ndarray:
-        """Predicted log(GB/s) for each row of X."""
-        out, _ = self.forward(self._norm(X))
-        return out.reshape(-1).cpu().numpy() * self.ysd + self.ymu
+        """Predicted log(GB/s) for each row of X (the mean over the ensemble's members)."""
+        Xn = self._norm(X)
+        out, _ = self.forward(Xn)
+        acc = out.reshape(-1).clone()
+        own = self.params
+        for params in self.extra:
+            self.params = params
+            try:
+                o, _ = self.forward(Xn)
+            finally:
+                self.params = own
+            acc += o.reshape(-1)
+        acc /= 1 + len(self.extra)
+        return acc.cpu().numpy() * self.ysd + self.ymu
 
     def save(self, path: Path, extra: Optional[dict] = None):
         path.parent.mkdir(parents=True, exist_ok=True)
         arrays = {f"p{i}": p.cpu().numpy() for i, p in enumerate(self.params)}
+        for k, params in enumerate(self.extra, start=1):
+            arrays.update({f"m{k}_p{i}": p.cpu().numpy() for i, p in enumerate(params)})
         meta = {"version": VERSION, "nin": self.nin, "hidden": self.hidden, "ymu": self.ymu, "ysd": self.ysd,
-                "rmse": self.rmse}
+                "rmse": self.rmse, "members": 1 + len(self.extra)}
         meta.update(extra or {})
         np.savez(path, mu=self.mu, sd=self.sd, meta=np.frombuffer(json.dumps(meta).encode(), np.uint8), **arrays)
 
@@ -308,6 +323,7 @@ class MLP:
             raise ValueError(f"cost model {path} has version {meta.get('version')}, expected {VERSION}")
         m = cls(meta["nin"], meta["hidden"])
         m.params = [torch.from_numpy(z[f"p{i}"]).cuda() for i in range(6)]
+        m.extra = [[torch.from_numpy(z[f"m{k}_p{i}"]).cuda() for i in range(6)] for k in range(1, meta.get("members", 1))]
         m.mu, m.sd = z["mu"], z["sd"]
         m.ymu, m.ysd, m.rmse = meta["ymu"], meta["ysd"], meta["rmse"]
         m.meta = meta
@@ -341,9 +357,11 @@ def numpy_forward_backward(params, X, y):
 
 
 def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batch: int = 2048, seed: int = 0,
-          val: float = 0.1, log=print, groups: Optional[np.ndarray] = None) -> MLP:
+          val: float = 0.1, log=print, groups: Optional[np.ndarray] = None, members: int = 1) -> MLP:
     """Fits log(GB/s) with the library's kernels. Holds out `val` of the rows for the RMSE (whole
-    problems when `groups` gives each row's problem)."""
+    problems when `groups` gives each row's problem). With members > 1, trains that many networks
+    from different initial weights on the same rows and returns them as one ensemble (predictions
+    averaged)."""
     import torch
     rng = np.random.default_rng(seed)
     val_groups = np.zeros(0, np.int64)
@@ -364,29 +382,42 @@ def train(X: np.ndarray, y: np.ndarray, epochs: int = 60, lr: float = 2e-3, batc
     m.ymu, m.ysd = float(y[ti].mean()), float(y[ti].std() + 1e-6)
     Xt = m._norm(X[ti])
     yt = torch.from_numpy(((y[ti] - m.ymu) / m.ysd).astype(np.float32)).cuda().reshape(-1, 1)
-    best_vr, best_params = float("inf"), None
-    for ep in range(epochs):
-        order = torch.from_numpy(rng.permutation(len(ti))).cuda()
-        tot = 0.0
-        for b0 in range(0, len(ti), batch):
-            sel = order[b0:b0 + batch]
-            xb, yb = Xt[sel].contiguous(), yt[sel].contiguous()
-            out, cache = m.forward(xb)
-            loss, d = m.loss_grad(out, yb)
-            grads = m.backward(d, cache)
-            m.step(grads, lr * (0.5 ** (ep // 20)))
-            tot += float(loss.item()) * len(sel)
+
+    def fit(net: MLP, order_rng) -> float:
+        """Trains one member; keeps the weights of its epoch with the lowest held-out error."""
+        best_vr, best_params = float("inf"), None
+        vr = float("nan")
+        for ep in range(epochs):
+            order = torch.from_numpy(order_rng.permutation(len(ti))).cuda()
+            tot = 0.0
+            for b0 in range(0, len(ti), batch):
+                sel = order[b0:b0 + batch]
+                xb, yb = Xt[sel].contiguous(), yt[sel].contiguous()
+                out, cache = net.forward(xb)
+                loss, d = net.loss_grad(out, yb)
+                grads = net.backward(d, cache)
+                net.step(grads, lr * (0.5 ** (ep // 20)))
+                tot += float(loss.item()) * len(sel)
+            if nval:
+                vr = float(np.sqrt(np.mean((net.predict(X[vi]) - y[vi]) ** 2)))
+                if vr < best_vr:
+                    best_vr, best_params = vr, [q.clone() for q in net.params]
+            if log and (ep % 10 == 0 or ep == epochs - 1):
+                log(f"epoch {ep}: train mse {tot / len(ti):.4f} (normalised), val rmse {vr:.4f} log(GB/s)")
         if nval:
-            # keep the weights of the epoch with the lowest held-out error (early stopping)
-            vr = float(np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)))
-            if vr < best_vr:
-                best_vr, best_params = vr, [q.clone() for q in m.params]
-        if log and (ep % 10 == 0 or ep == epochs - 1):
-            log(f"epoch {ep}: train mse {tot / len(ti):.4f} (normalised), val rmse "
-                f"{vr if nval else float('nan'):.4f} log(GB/s)")
+            net.params = best_params
+        return best_vr
+
+    fit(m, rng)
+    for k in range(1, members):
+        net = MLP(X.shape[1], 128, seed + k)
+        net.mu, net.sd, net.ymu, net.ysd = m.mu, m.sd, m.ymu, m.ysd
+        if log:
+            log(f"member {k}")
+        fit(net, np.random.default_rng(seed + 1000 * k))
+        m.extra.append(net.params)
     if nval:
-        m.params = best_params
-        m.rmse = best_vr
+        m.rmse = float(np.sqrt(np.mean((m.predict(X[vi]) - y[vi]) ** 2)))
     return m
 
 
@@ -424,7 +455,7 @@ def load_default(path: Optional[Path] = None) -> MLP:
 # POLICY["lo"] the default stays. On the 500 held-out problems' stored timings, timing the top 1, 2
 # or 3 with the default kept 0.952, 0.964 and 0.971 of the best measured GB/s (the default alone
 # 0.925). `train` fits the thresholds on its held-out problems and stores them with the model.
-DEFAULT_POLICY = {"lo": 0.02, "hi": 0.3, "k": 2}
+DEFAULT_POLICY = {"lo": 0.02, "hi": 0.3, "k": 2}  # a trained model stores its own (lo, hi, k)
 
 
 def policy_of(model) -> dict:
@@ -695,6 +726,7 @@ def main(argv=None):
     ap.add_argument("--model", default=str(DEFAULT_MODEL))
     ap.add_argument("--max-impl", type=int, default=64)
     ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--members", type=int, default=5, help="train: networks in the ensemble")
     ap.add_argument("--out-json", default=None)
     ap.add_argument("--max-seconds", type=float, default=None, help="collect: stop (resumably) after this long")
     a = ap.parse_args(argv)
@@ -708,7 +740,7 @@ def main(argv=None):
         z = np.load(train_path)
         X, case = corpus_features(json.loads(bytes(z["meta"]).decode()))
         meta = json.loads(bytes(z["meta"]).decode())
-        m = train(X, z["y"], epochs=a.epochs, groups=case)
+        m = train(X, z["y"], epochs=a.epochs, groups=case, members=a.members)
         # the policy thresholds, fitted on the training run's held-out problems
         held = np.isin(case, m.val_groups)
         policy = fit_policy(m.predict(X[held]), z["y"][held], case[held], meta) if held.any() else DEFAULT_POLICY
