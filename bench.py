@@ -7,6 +7,9 @@ A step = one pass over the 64-case sweep: seeded rank-2..6 transpositions with |
 same 64 cases through the public call with pinned host buffers and the host<->device copies inside
 the timed region, beside the PCIe bandwidth measured in the same run. The CPU baseline (TTC's own
 generated AVX code, rebuilt for this host with TTC's Makefile flags) runs the same 64 cases.
+Each case is timed with the schedule that a measured search picked for it before the timed region
+(TTC's method: every candidate timed and checked against the first); `schedule_kinds` gives the sweep
+under the planner's defaults and the learned selector's choices too, with each one's tuning time.
 On one GPU the line also carries the other configurations: the README shape, the strided mixed-
 precision shapes, the batched workload against per-call launches, and the learned selector against
 a fresh measured search on held-out problems.
@@ -65,11 +68,16 @@ def parse(argv=None):
                          "--reps times with its default plan (a small command for profilers); configs: the "
                          "README shape and the strided mixed-precision shapes, each timed alone; batchcase: the "
                          "batched workload with the planner's schedules launched --reps times (for profilers)")
-    ap.add_argument("--schedule", default="learned", choices=["default", "learned"],
-                    help="sweep: the planner's default schedule per case, or the learned selector's choice "
-                         "(chosen before the timed region: its top-1 on a large predicted gain over the "
-                         "planner default, the fastest of its top candidates and the default, timed, on a "
-                         "moderate one)")
+    ap.add_argument("--schedule", default="search", choices=["search", "learned", "default"],
+                    help="sweep: the schedule each case is timed with, chosen before the timed region. "
+                         "search: TTC's method, every candidate schedule (up to --search-candidates) timed "
+                         "and checked bit for bit against the first, the fastest kept; learned: the learned "
+                         "selector (its top-1 on a large predicted gain over the planner default, the "
+                         "fastest of its top candidates and the default, timed, on a moderate one); "
+                         "default: the planner's. Unless --no-extras, the other two are timed as well and "
+                         "reported beside it")
+    ap.add_argument("--search-candidates", type=int, default=64,
+                    help="sweep: candidate schedules per case for the measured search")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
     ap.add_argument("--reps", type=int, default=3, help="case / batchcase: launches")
     ap.add_argument("--tuning", default=None, help="case: a schedule (JSON of ttcb_tuning fields) instead of the "
@@ -499,32 +507,47 @@ def run_sweep(args, rank, world, local):
     # the learned selector needs its trained model; without one the planner's defaults are timed
     # and the line says so
     schedule_note = None
-    if args.schedule == "learned":
-        try:
-            from ttc_b200 import cost_model
-            cost_model.load_default()
-        except Exception as ex:
+    learned_ok = True
+    try:
+        from ttc_b200 import cost_model
+        cost_model.load_default()
+    except Exception as ex:
+        learned_ok = False
+        if args.schedule == "learned":
             args.schedule = "default"
             schedule_note = f"learned model unavailable ({type(ex).__name__}: {ex}); planner defaults timed"
+    # the headline's schedules first, then (unless --no-extras) the other kinds for the comparison
+    sched_kinds = [args.schedule] + ([k for k in ("default", "learned", "search")
+                                if k != args.schedule and (k != "learned" or learned_ok)]
+                               if not args.no_extras else [])
+
+    def choose(kind, c):
+        from ttc_b200.autotune import Problem, search
+        p = Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"])
+        if kind == "learned":
+            return cost_model.choose_tuning(p)
+        if kind == "search":
+            r = search(p, max_impl=args.search_candidates, reps=3, verify=True, seed=c["seed"])
+            torch.cuda.empty_cache()
+            return dict(r["best"].tuning) or None
+        return None
 
     # resident inputs, seeded on the device
     gen = torch.Generator(device=dev)
     items = []
-    t_sel = 0.0
+    tunings = {k: [] for k in sched_kinds}
+    t_sel = {k: 0.0 for k in sched_kinds}
     for c in cases:
         n = math.prod(c["size"])
         gen.manual_seed(c["seed"])
         A = torch.rand(n, dtype=tmap[c["dtype"]], device=dev, generator=gen).mul_(2).sub_(1)
         gen.manual_seed(c["seed"] + 1)
         B = torch.rand(n, dtype=tmap[c["dtype"]], device=dev, generator=gen).mul_(2).sub_(1)
-        tuning = None
-        if args.schedule == "learned":
-            from ttc_b200 import cost_model
-            from ttc_b200.autotune import Problem
+        for k in sched_kinds:
             t0 = time.perf_counter()
-            tuning = cost_model.choose_tuning(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]))
-            t_sel += time.perf_counter() - t0
-        plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=tuning)
+            tunings[k].append(choose(k, c))
+            t_sel[k] += time.perf_counter() - t0
+        plan = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=tunings[args.schedule][-1])
         items.append((c, plan, A, B))
     torch.cuda.synchronize()
     bytes_per_step = sum(p.bytes for _, p, _, _ in items)
@@ -596,6 +619,21 @@ def run_sweep(args, rank, world, local):
                           for k, v in per_kind.items()},
                 "per_case_GBps": per_case, "cases_below_0.7_of_peak": int(sum(g < 0.7 * peak for g in per_case))}
 
+    # the other kinds of schedule on the same resident inputs, timed the same way (back to back)
+    schedule_kinds = {args.schedule: {"GBps": round(value, 1), "ms_per_step": round(ms_per_step, 4),
+                                      "tuning_seconds": round(t_sel[args.schedule], 1)}}
+    for k in sched_kinds[1:]:
+        alt = [(c, Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning=tu), A, B)
+               for (c, _, A, B), tu in zip(items, tunings[k])]
+        ms_k = sweep_pass_ms(alt, args.steps, args.warmup, stream, dev, world)
+        schedule_kinds[k] = {"GBps": round(job_throughput(bytes_per_step, world, ms_k), 1),
+                             "ms_per_step": round(ms_k, 4), "tuning_seconds": round(t_sel[k], 1)}
+        for _, p, _, _ in alt:
+            p.close()
+    for k in sched_kinds:
+        if k != "default":
+            schedule_kinds[k]["cases_off_default"] = sum(1 for tu in tunings[k] if tu)
+
     # end to end through the public call with pinned host buffers, over the same cases
     pcie = measure_pcie(dev) if rank == 0 or world > 1 else None
     e2e, host = run_e2e(args, items, stream, dev, world, pcie)
@@ -630,10 +668,9 @@ def run_sweep(args, rank, world, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded uniform[-1,1])",
                 "pct_of_hbm_peak": round(100 * value / world / peak, 2),
                 "config": sweep_config(len(cases), bytes_per_step, world),
-                "schedules": schedule_note or ("learned selector (top-1 on a large predicted gain over the planner "
-                                               "default; its top candidates timed against it on a moderate one)" if args.schedule == "learned"
-                                               else "planner default"),
-                "schedule_seconds": round(t_sel, 1),
+                "schedules": schedule_note or SCHEDULE_NOTES[args.schedule],
+                "schedule_seconds": round(t_sel[args.schedule], 1),
+                "schedule_kinds": schedule_kinds,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches_per_step * args.steps, **extras}
         print(json.dumps(line), flush=True)
@@ -641,6 +678,39 @@ def run_sweep(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+SCHEDULE_NOTES = {
+    "search": ("measured search per case (TTC's method): up to 64 candidate schedules (tile shape x raster x "
+               "ring depth and CTAs per SM x tile order x copy form) each timed, best of 3, and checked bit for "
+               "bit against the first; the fastest kept. Chosen before the timed region"),
+    "learned": ("learned selector (top-1 on a large predicted gain over the planner default; its top candidates "
+                "timed against it on a moderate one). Chosen before the timed region"),
+    "default": "planner default",
+}
+
+
+def sweep_pass_ms(items, steps, warmup, stream, dev, world):
+    """ms per pass over `items` [(case, plan, A, B)], back to back with CUDA events after `warmup`
+    untimed passes; the maximum over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    def one():
+        for c, plan, A, B in items:
+            plan(A, B, c["alpha"], c["beta"], stream)
+    for _ in range(warmup):
+        one()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return max_over_ranks(e0.elapsed_time(e1), dev) / steps
 
 
 # ------------------------------------------------------------------------------------------------

@@ -2,11 +2,12 @@
 
 Every case of the 64-case sweep that the benchmark times (seed 2024: rank 2..6, fp32/fp64, |A| ~
 200 MiB, one extent in [7, 31]; even cases alpha = 1 beta = 0, odd cases alpha = 1.5 beta = -0.5) runs
-through the public Plan call with the planner's default schedule and with the learned selector's
-schedule (the one the benchmark uses), on the benchmark's own seeded device inputs, and is compared
-bit for bit with the oracle: the restated reference loop of TTC's CUDA path (GPUreference.py:90-137
+through the public Plan call with the planner's default schedule, with the learned selector's
+schedule and with the measured search's winner (the benchmark's headline schedule), on the benchmark's
+own seeded device inputs, and is compared bit for bit with the oracle: the restated reference loop of TTC's CUDA path (GPUreference.py:90-137
 in the TTC project), in its OpenMP form. A canary after B catches writes past its end. Cases run one
-at a time, so the device holds one case's A, B and result at once.
+at a time, so the device holds one case's A, B and result at once. The search itself compares every
+candidate's output bit for bit with its first candidate's (the planner default's shape).
 """
 import math
 import os
@@ -35,7 +36,7 @@ def _inputs(c, dev):
     return A, B
 
 
-@pytest.mark.parametrize("schedule", ["default", "learned"])
+@pytest.mark.parametrize("schedule", ["default", "learned", "search"])
 def test_sweep64_full_size_matches_oracle(schedule):
     import torch
     import ttc_b200.workloads as wl
@@ -52,6 +53,14 @@ def test_sweep64_full_size_matches_oracle(schedule):
             tuning = cost_model.choose_tuning(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]))
             if tuning is None:
                 continue  # the planner default, checked by the other schedule
+        elif schedule == "search":
+            from ttc_b200.autotune import search
+            r = search(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"]), max_impl=64, reps=1,
+                       verify=True, seed=c["seed"])
+            torch.cuda.empty_cache()
+            tuning = dict(r["best"].tuning) or None
+            if tuning is None:
+                continue
         A, B = _inputs(c, dev)
         n = A.numel()
         hA = A.cpu().numpy()
