@@ -633,6 +633,7 @@ def run_sweep(args, rank, world, local):
     for k in sched_kinds:
         if k != "default":
             schedule_kinds[k]["cases_off_default"] = sum(1 for tu in tunings[k] if tu)
+            schedule_kinds[k]["knobs"] = knob_counts(tunings[k])
 
     # end to end through the public call with pinned host buffers, over the same cases
     pcie = measure_pcie(dev) if rank == 0 or world > 1 else None
@@ -688,6 +689,17 @@ SCHEDULE_NOTES = {
                 "timed against it on a moderate one). Chosen before the timed region"),
     "default": "planner default",
 }
+
+
+def knob_counts(tunings) -> dict:
+    """How many of the cases' schedules set each ttcb_tuning field, with the values that matter for
+    the copy form and the tile order (bulk A copies, shifted runs, claimed or round-robin tiles)."""
+    out = {}
+    for tu in tunings:
+        for key, val in (tu or {}).items():
+            name = f"{key}={val}" if key in ("bulk_copies", "shifted_runs", "round_robin", "lane_map") else key
+            out[name] = out.get(name, 0) + 1
+    return dict(sorted(out.items()))
 
 
 def sweep_pass_ms(items, steps, warmup, stream, dev, world):
