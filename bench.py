@@ -76,8 +76,9 @@ def parse(argv=None):
                          "fastest of its top candidates and the default, timed, on a moderate one); "
                          "default: the planner's. Unless --no-extras, the other two are timed as well and "
                          "reported beside it")
-    ap.add_argument("--search-candidates", type=int, default=64,
-                    help="sweep: candidate schedules per case for the measured search")
+    ap.add_argument("--search-candidates", type=int, default=200,
+                    help="sweep: candidate schedules per case for the measured search (TTC's default "
+                         "maxImplementations; the sweep's cases have 1 to 112 candidates, 49 on average)")
     ap.add_argument("--case", type=int, default=6, help="case: index into the sweep")
     ap.add_argument("--reps", type=int, default=3, help="case / batchcase: launches")
     ap.add_argument("--tuning", default=None, help="case: a schedule (JSON of ttcb_tuning fields) instead of the "
@@ -682,8 +683,8 @@ def run_sweep(args, rank, world, local):
 
 
 SCHEDULE_NOTES = {
-    "search": ("measured search per case (TTC's method): up to 64 candidate schedules (tile shape x raster x "
-               "ring depth and CTAs per SM x tile order x copy form) each timed, best of 3, and checked bit for "
+    "search": ("measured search per case (TTC's method): every candidate schedule (tile shape x raster x ring "
+               "depth and CTAs per SM x tile order x copy form; up to 200) timed, best of 3, and checked bit for "
                "bit against the first; the fastest kept. Chosen before the timed region"),
     "learned": ("learned selector (top-1 on a large predicted gain over the planner default; its top candidates "
                 "timed against it on a moderate one). Chosen before the timed region"),
