@@ -32,6 +32,10 @@ ttcb_status ttcb_mlp_mse(const float* pred, const float* target, int n, float* d
 ttcb_status ttcb_mlp_adam(float* param, const float* grad, float* m, float* v, int n, float lr, float beta1,
                           float beta2, float eps, int t, ttcb_stream_t stream);
 
+/* The same step with L2 weight decay: the gradient used is grad + weight_decay * param. */
+ttcb_status ttcb_mlp_adam_l2(float* param, const float* grad, float* m, float* v, int n, float lr, float beta1,
+                             float beta2, float eps, float weight_decay, int t, ttcb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,28 @@ def test_adam_step_matches_formula():
     assert np.allclose(tp.cpu().numpy(), p, rtol=1e-5, atol=1e-6)
 
 
+def test_adam_step_with_weight_decay_matches_formula():
+    import torch
+    from ttc_b200 import _native
+    from ttc_b200.cost_model import _lib
+    rng = np.random.default_rng(7)
+    p = rng.standard_normal(1000).astype(np.float32)
+    g = rng.standard_normal(1000).astype(np.float32)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    tp, tg, tm, tv = (torch.from_numpy(x.copy()).cuda() for x in (p, g, m, v))
+    wd = 0.01
+    for t in (1, 2, 3):
+        _native.check(_lib().ttcb_mlp_adam_l2(tp.data_ptr(), tg.data_ptr(), tm.data_ptr(), tv.data_ptr(), 1000,
+                                              0.01, 0.9, 0.999, 1e-8, wd, t,
+                                              torch.cuda.current_stream().cuda_stream))
+        ge = g + wd * p
+        m = 0.9 * m + 0.1 * ge
+        v = 0.999 * v + 0.001 * ge * ge
+        p = p - 0.01 * (m / (1 - 0.9 ** t)) / (np.sqrt(v / (1 - 0.999 ** t)) + 1e-8)
+    assert np.allclose(tp.cpu().numpy(), p, rtol=1e-5, atol=1e-6)
+
+
 def test_training_fits_a_smooth_function():
     from ttc_b200.cost_model import train
     rng = np.random.default_rng(6)

@@ -112,11 +112,12 @@ __global__ void mse_kernel(const float* __restrict__ pred, const float* __restri
   if (threadIdx.x == 0) atomicAdd(loss, red[0] / (float)n);
 }
 
+// wd: L2 weight decay, added to the gradient before the moments (wd * p).
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
-                            float c2) {
+                            float c2, float wd) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float gi = g[i];
+    const float gi = g[i] + wd * p[i];
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
@@ -172,13 +173,18 @@ ttcb_status ttcb_mlp_mse(const float* pred, const float* target, int n, float* d
   return check_launch("ttcb_mlp_mse");
 }
 
-ttcb_status ttcb_mlp_adam(float* param, const float* grad, float* m, float* v, int n, float lr, float beta1,
-                          float beta2, float eps, int t, ttcb_stream_t stream) {
+ttcb_status ttcb_mlp_adam_l2(float* param, const float* grad, float* m, float* v, int n, float lr, float beta1,
+                             float beta2, float eps, float weight_decay, int t, ttcb_stream_t stream) {
   if (n <= 0) return TTCB_OK;
   const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
   adam_kernel<<<grid_for(n), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(param, grad, m, v, n, lr, beta1,
-                                                                               beta2, eps, c1, c2);
+                                                                               beta2, eps, c1, c2, weight_decay);
   return check_launch("ttcb_mlp_adam");
+}
+
+ttcb_status ttcb_mlp_adam(float* param, const float* grad, float* m, float* v, int n, float lr, float beta1,
+                          float beta2, float eps, int t, ttcb_stream_t stream) {
+  return ttcb_mlp_adam_l2(param, grad, m, v, n, lr, beta1, beta2, eps, 0.f, t, stream);
 }
 
 }  // extern "C"
