@@ -28,3 +28,18 @@ def test_describe_launches_counts_edge_plans():
     assert describe_launches(parent) == 1 + 1 + 2
     legacy = dict(parent, tile_variant=1)  # the legacy kernels move ragged tiles inline
     assert describe_launches(legacy) == 1
+
+
+def test_knob_counts_and_schedule_kinds():
+    """The sweep line's `schedule_kinds` counts, per kind of schedule, the cases whose schedule sets
+    each tuning field (copy form and tile order with their values), and every kind has its note."""
+    import bench
+    tunings = [None, {"bulk_copies": 1, "stages": 4}, {"round_robin": -1, "stages": 5},
+               {"shifted_runs": 1, "bulk_copies": 1}, {}]
+    assert bench.knob_counts(tunings) == {"bulk_copies=1": 2, "round_robin=-1": 1, "shifted_runs=1": 1,
+                                          "stages": 2}
+    assert bench.knob_counts([None, {}]) == {}
+    args = bench.parse([])
+    assert args.schedule == "search" and args.search_candidates == 200
+    assert set(bench.SCHEDULE_NOTES) == {"search", "learned", "default"}
+    assert bench.parse(["--schedule", "learned"]).schedule == "learned"
