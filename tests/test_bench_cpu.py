@@ -43,3 +43,28 @@ def test_knob_counts_and_schedule_kinds():
     assert args.schedule == "search" and args.search_candidates == 200
     assert set(bench.SCHEDULE_NOTES) == {"search", "learned", "default"}
     assert bench.parse(["--schedule", "learned"]).schedule == "learned"
+
+
+def test_sweep_schedule_rules():
+    """The schedule-comparison presets (host planning only): bulk copies are asked for only where
+    the planner can make them, the bytes per bulk copy follow the staged layout's pieces, and the
+    320-byte rule keeps the long copies."""
+    from ttc_b200 import sweep_schedules as ss
+    from ttc_b200.core import plan_host_json
+    from ttc_b200.workloads import sweep_cases
+    cases = sweep_cases(2024)
+    rules = ss.PRESETS["bulk"]
+    assert rules["default"](cases[0]) is None
+    assert rules["round_robin"](cases[0]) == {"round_robin": 1}
+    for c in cases:
+        d = plan_host_json(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning={"bulk_copies": 1})
+        nb = ss.bulk_copy_bytes(d, c["dtype"])
+        assert nb == 0 or nb % 16 == 0, (c, nb)  # whole 16-byte vectors
+        long_rule = rules["bulk_320"](c)
+        assert (long_rule == {"bulk_copies": 1}) == (nb >= ss.BULK_MIN_BYTES), (c, nb, long_rule)
+    # sweep case 25 (fp64, runs of 96 elements, one bulk copy per run) and case 6 (fp64, 1920-element
+    # runs cut into 40-element pieces at the padding points)
+    for k, want in ((25, 768), (6, 320)):
+        c = cases[k]
+        d = plan_host_json(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning={"bulk_copies": 1})
+        assert ss.bulk_copy_bytes(d, c["dtype"]) == want
