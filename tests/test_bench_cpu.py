@@ -55,6 +55,8 @@ def test_sweep_schedule_rules():
     cases = sweep_cases(2024)
     rules = ss.PRESETS["bulk"]
     assert rules["default"](cases[0]) is None
+    assert ss.PRESETS["tile_order"]["group_3"](cases[0]) == {"claim_group": 3}
+    assert ss.PRESETS["lane_maps"]["lane_map"](cases[0]) == {"lane_map": 1}
     assert rules["round_robin"](cases[0]) == {"round_robin": 1}
     for c in cases:
         d = plan_host_json(c["perm"], c["size"], c["dtype"], c["beta"] != 0, tuning={"bulk_copies": 1})

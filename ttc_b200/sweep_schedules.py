@@ -1,6 +1,6 @@
 """Times the 64-case 200 MiB sweep under several per-case schedule rules, on one GPU.
 
-    python -m ttc_b200.sweep_schedules --preset bulk [--repeats 2] [--seed 2024]
+    python -m ttc_b200.sweep_schedules --preset bulk|tile_order|lane_maps [--repeats 2] [--seed 2024]
 
 The sweep is the benchmark's (`ttc_b200.workloads.sweep_cases`: seeded rank-2..6 fp32/fp64
 transpositions, |A| ~ 200 MiB, half with alpha = 1.5, beta = -0.5). Inputs are seeded on the device
@@ -67,6 +67,22 @@ PRESETS = {
         "round_robin": _fixed({"round_robin": 1}),
         "round_robin_bulk": _fixed({"round_robin": 1, "bulk_copies": 1}),
         "round_robin_bulk_320": _bulk_if_long({"round_robin": 1}),
+    },
+    # the staged kernel's tile order: the planner's claims rule with 1, 2 (its default), 3 or 4 tiles
+    # per claim, claims for every tile plan, round robin everywhere
+    "tile_order": {
+        "default": _fixed({}),
+        "group_1": _fixed({"claim_group": 1}),
+        "group_3": _fixed({"claim_group": 3}),
+        "group_4": _fixed({"claim_group": 4}),
+        "claims": _fixed({"round_robin": -1}),
+        "claims_group_4": _fixed({"round_robin": -1, "claim_group": 4}),
+        "round_robin": _fixed({"round_robin": 1}),
+    },
+    # the register path's lane maps (a warp's B vectors taken from several B runs)
+    "lane_maps": {
+        "default": _fixed({}),
+        "lane_map": _fixed({"lane_map": 1}),
     },
 }
 
