@@ -1,6 +1,8 @@
 """Times the 64-case 200 MiB sweep under several per-case schedule rules, on one GPU.
 
-    python -m ttc_b200.sweep_schedules --preset bulk|tile_order|lane_maps [--repeats 2] [--seed 2024]
+    python -m ttc_b200.sweep_schedules --preset PRESET [--repeats 2] [--seed 2024]
+
+PRESET: bulk, tile_order, lane_maps, shifted_runs or ring_depth (see PRESETS).
 
 The sweep is the benchmark's (`ttc_b200.workloads.sweep_cases`: seeded rank-2..6 fp32/fp64
 transpositions, |A| ~ 200 MiB, half with alpha = 1.5, beta = -0.5). Inputs are seeded on the device
@@ -83,6 +85,19 @@ PRESETS = {
     "lane_maps": {
         "default": _fixed({}),
         "lane_map": _fixed({"lane_map": 1}),
+    },
+    # A runs that 16-byte copies cannot reach, copied as the 16-byte chunks that cover them
+    "shifted_runs": {
+        "default": _fixed({}),
+        "shifted_runs": _fixed({"shifted_runs": 1}),
+    },
+    # the ring depth: the planner's rule (tiles in motion nearest 18 MiB) against fixed depths
+    "ring_depth": {
+        "default": _fixed({}),
+        "stages_3": _fixed({"stages": 3}),
+        "stages_4": _fixed({"stages": 4}),
+        "stages_5": _fixed({"stages": 5}),
+        "stages_6": _fixed({"stages": 6}),
     },
 }
 
