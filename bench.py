@@ -635,6 +635,7 @@ def run_sweep(args, rank, world, local):
         if k != "default":
             schedule_kinds[k]["cases_off_default"] = sum(1 for tu in tunings[k] if tu)
             schedule_kinds[k]["knobs"] = knob_counts(tunings[k])
+            schedule_kinds[k]["per_case"] = [tu or {} for tu in tunings[k]]
 
     # end to end through the public call with pinned host buffers, over the same cases
     pcie = measure_pcie(dev) if rank == 0 or world > 1 else None
