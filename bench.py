@@ -635,7 +635,7 @@ def run_sweep(args, rank, world, local):
         if k != "default":
             schedule_kinds[k]["cases_off_default"] = sum(1 for tu in tunings[k] if tu)
             schedule_kinds[k]["knobs"] = knob_counts(tunings[k])
-            schedule_kinds[k]["per_case"] = [tu or {} for tu in tunings[k]]
+            schedule_kinds[k]["per_case"] = [plain_json(tu or {}) for tu in tunings[k]]
 
     # end to end through the public call with pinned host buffers, over the same cases
     pcie = measure_pcie(dev) if rank == 0 or world > 1 else None
@@ -691,6 +691,11 @@ SCHEDULE_NOTES = {
                 "timed against it on a moderate one). Chosen before the timed region"),
     "default": "planner default",
 }
+
+
+def plain_json(x):
+    """`x` with numpy scalars turned into Python numbers, so that json.dumps takes it."""
+    return json.loads(json.dumps(x, default=lambda o: o.item() if hasattr(o, "item") else str(o)))
 
 
 def knob_counts(tunings) -> dict:

@@ -39,6 +39,8 @@ def test_knob_counts_and_schedule_kinds():
     assert bench.knob_counts(tunings) == {"bulk_copies=1": 2, "round_robin=-1": 1, "shifted_runs=1": 1,
                                           "stages": 2}
     assert bench.knob_counts([None, {}]) == {}
+    import numpy as np
+    assert bench.plain_json({"stages": np.int64(4), "raster": [np.int32(2), 1]}) == {"stages": 4, "raster": [2, 1]}
     args = bench.parse([])
     assert args.schedule == "search" and args.search_candidates == 200
     assert set(bench.SCHEDULE_NOTES) == {"search", "learned", "default"}
