@@ -806,6 +806,23 @@ def configs_summary(args, steps=None, warmup=None):
             lp.close()
         elif "learned" not in out[name]:
             out[name]["learned"] = {"tuning": {}, "note": "the selector kept the planner default"}
+        # the measured search's winner (TTC's method, as the sweep's `value` uses it)
+        try:
+            from ttc_b200.autotune import Problem, search
+            t0 = time.perf_counter()
+            r = search(Problem(c["perm"], c["size"], c["dtype"], c["alpha"], c["beta"], c.get("lda")),
+                       max_impl=args.search_candidates, reps=3, verify=True, seed=args.seed)
+            secs = time.perf_counter() - t0
+            stu = plain_json(dict(r["best"].tuning))
+            sp = Plan(c["perm"], c["size"], c["dtype"], c["beta"] != 0, lda=c.get("lda"), tuning=stu or None)
+            smed, sbest = flushed_timing(sp, A, B, c["alpha"], c["beta"], steps, warmup, flush)
+            sg = sp.bytes / (smed / 1e3) / 1e9
+            out[name]["search"] = {"tuning": stu, "candidates": r["candidates"], "tuning_seconds": round(secs, 2),
+                                   "GBps_median": round(sg, 1), "frac_of_hbm_peak": round(sg / peak, 4)}
+            sp.close()
+        except Exception as ex:  # reported, never required
+            out[name]["search"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        torch.cuda.empty_cache()
     return out
 
 
